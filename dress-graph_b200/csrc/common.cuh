@@ -1,0 +1,148 @@
+// common.cuh -- device helpers shared by the B200 DRESS kernels.
+//
+// Exactness rules (all kernels are compiled with --fmad=false as well):
+//   * every product and sum uses the explicit round-to-nearest intrinsics,
+//     so no multiply-add is ever fused;
+//   * every multi-term sum is "sort ascending, then sequential
+//     Kahan-Babuska-Neumaier" exactly as the reference does it
+//     (libdress/src/dress.c:51-66), which makes the result independent of
+//     the order in which the terms were gathered;
+//   * sqrt and division are the IEEE round-to-nearest forms.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define DRESS_INF __longlong_as_double(0x7ff0000000000000ULL)
+
+namespace dress {
+
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dsqrt(double a) { return __dsqrt_rn(a); }
+
+// One Neumaier step: s <- s + b with the lost low part accumulated in c.
+__device__ __forceinline__ void kbn_step(double &s, double &c, double b)
+{
+    double t = dadd(s, b);
+    double e = (fabs(s) >= fabs(b)) ? dadd(dsub(s, t), b) : dadd(dsub(b, t), s);
+    c = dadd(c, e);
+    s = t;
+}
+
+// Compare-exchange putting the smaller value at the lower position.
+__device__ __forceinline__ void cswap(double &a, double &b)
+{
+    bool sw = b < a;
+    double lo = sw ? b : a;
+    double hi = sw ? a : b;
+    a = lo;
+    b = hi;
+}
+
+// Register sorting network on M (power of two) values, ascending.  Bitonic
+// network in its single-direction form: for every block size k the first
+// comparator pairs i with its mirror i^(k-1), the rest pair i with i^j.
+// Missing values are padded with +inf by the caller.
+template <int M>
+__device__ __forceinline__ void sort_regs(double (&a)[M])
+{
+#pragma unroll
+    for (int k = 2; k <= M; k <<= 1) {
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            int j = i ^ (k - 1);
+            if (j > i) cswap(a[i], a[j]);
+        }
+#pragma unroll
+        for (int s = k >> 2; s > 0; s >>= 1) {
+#pragma unroll
+            for (int i = 0; i < M; ++i) {
+                int j = i ^ s;
+                if (j > i) cswap(a[i], a[j]);
+            }
+        }
+    }
+}
+
+// Sorted KBN over the first n (1 <= n <= M) register values.
+template <int M>
+__device__ __forceinline__ double kbn_regs(const double (&a)[M], int n)
+{
+    double s = a[0], c = 0.0;
+#pragma unroll
+    for (int i = 1; i < M; ++i)
+        if (i < n) kbn_step(s, c, a[i]);
+    return dadd(s, c);
+}
+
+// Cooperative in-place ascending sort of buf[0..n) by `nthr` threads with
+// index `tid` (a warp or a whole block).  Same single-direction bitonic
+// network over the next power of two; comparators whose upper index is
+// >= n would compare against a virtual +inf and are skipped.  `sync` is the
+// barrier of the cooperating group.
+template <class Sync>
+__device__ __forceinline__ void sort_shared(double *buf, int n, int tid, int nthr, Sync sync)
+{
+    int M = 1;
+    while (M < n) M <<= 1;
+    for (int k = 2; k <= M; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            // each comparator is identified by its lower index i with bit j clear
+            int half = M >> 1;
+            for (int q = tid; q < half; q += nthr) {
+                int i = ((q & ~(j - 1)) << 1) | (q & (j - 1));   // insert a 0 at bit j
+                int p = (j == (k >> 1)) ? (i ^ (k - 1)) : (i | j);
+                int lo = i < p ? i : p, hi = i < p ? p : i;
+                if (hi < n) {
+                    double x = buf[lo], y = buf[hi];
+                    if (y < x) { buf[lo] = y; buf[hi] = x; }
+                }
+            }
+            sync();
+        }
+    }
+}
+
+// Sequential sorted-KBN over buf[0..n), n >= 1.
+__device__ __forceinline__ double kbn_sorted_buf(const double *buf, int n)
+{
+    double s = buf[0], c = 0.0;
+    int i = 1;
+    for (; i + 4 <= n; i += 4) {
+        double b0 = buf[i], b1 = buf[i + 1], b2 = buf[i + 2], b3 = buf[i + 3];
+        kbn_step(s, c, b0);
+        kbn_step(s, c, b1);
+        kbn_step(s, c, b2);
+        kbn_step(s, c, b3);
+    }
+    for (; i < n; ++i) kbn_step(s, c, buf[i]);
+    return dadd(s, c);
+}
+
+// Max of a non-negative double over a block, folded into *dst (bits of a
+// non-negative double order like unsigned integers).  NaN and 0 are ignored,
+// as in the reference's `if (d > max_delta)` update.
+__device__ __forceinline__ void block_max_to(unsigned long long *dst, double v)
+{
+    __shared__ double red[32];
+    if (!(v > 0.0)) v = 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? red[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0 && v > 0.0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+__device__ __forceinline__ bool iteration_skipped(const unsigned long long *maxd, int iter, double eps)
+{
+    return iter > 0 && __longlong_as_double((long long)maxd[iter - 1]) < eps;
+}
+
+}  // namespace dress

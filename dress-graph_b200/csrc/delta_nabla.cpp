@@ -1,0 +1,740 @@
+// delta_nabla.cpp -- Delta^k / Nabla^k requests and the legacy entry points.
+//
+// Reference drivers: libdress/src/delta_dress_impl.c:171-318 and
+// libdress/src/nabla_dress_impl.c:142-311; public wrappers
+// libdress/src/cuda/delta_dress_cuda.c:24-85, nabla_dress_cuda.c:24-85.
+// The argument meaning is unchanged: subsets (ordered tuples) are ranked
+// lexicographically, rank s is processed when s % stride == offset, with
+// n_samples > 0 a sorted, de-duplicated LCG sample of the stride's ranks is
+// processed, k == 0 fits the caller's graph in place, k >= N gives an empty
+// histogram, edgeless subgraphs are skipped, and the histogram is the exact
+// (value, count) list ascending by value.
+//
+// Requests whose parent fits the batched kernel (rows of at most 31
+// neighbours, per-subgraph state within shared memory) are packed into one
+// persistent launch; any other request runs through the per-subgraph path:
+// host-built subgraph + single-graph GPU fit (the reference's structure,
+// which is also the "plain per-fit launch loop" the batched engine is
+// measured against).  Histograms are always built on the GPU.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "batch.h"
+#include "engine.h"
+#include "hist.h"
+
+namespace dress {
+namespace {
+
+long long binom_h(int n, int k)
+{
+    if (k < 0 || k > n) return 0;
+    if (k == 0 || k == n) return 1;
+    if (k > n - k) k = n - k;
+    long long r = 1;
+    for (int i = 0; i < k; ++i) r = r * (n - i) / (i + 1);
+    return r;
+}
+
+long long perm_h(int n, int k)
+{
+    if (k < 0 || k > n) return 0;
+    long long r = 1;
+    for (int i = 0; i < k; ++i) r *= (n - i);
+    return r;
+}
+
+int lcg15(unsigned int *s)
+{
+    *s = *s * 1103515245u + 12345u;
+    return (int)((*s >> 16) & 0x7fff);
+}
+
+// Sampled positions within the stride: n draws of a 62-bit LCG value
+// (first draw in the high part) modulo the stride's size, sorted and
+// de-duplicated (libdress/src/delta_dress_impl.c:153-157, 234-254).
+std::vector<long long> sample_picks(long long per, int n, unsigned int seed, int offset)
+{
+    long long lim = n < per ? n : per;
+    std::vector<long long> p((size_t)lim);
+    unsigned int s = seed + (unsigned int)offset;
+    for (long long i = 0; i < lim; ++i) {
+        long long hi = lcg15(&s);
+        long long lo = lcg15(&s);
+        p[(size_t)i] = (((hi << 31) | lo) & 0x7FFFFFFFFFFFFFFFLL) % per;
+    }
+    std::sort(p.begin(), p.end());
+    p.erase(std::unique(p.begin(), p.end()), p.end());
+    return p;
+}
+
+inline int next_pow2(int x)
+{
+    int m = 1;
+    while (m < x) m <<= 1;
+    return m;
+}
+
+// Everything one request needs, prepared on the host.
+struct Prep {
+    dressx_hist_request_t *r = nullptr;
+    p_dress_graph_t g = nullptr;
+    int N = 0, E = 0, S = 0, T = 0;
+    long long total = 0;               // C(N,k) or P(N,k)
+    long long per = 0;                 // ranks in this stride
+    std::vector<long long> ranks;      // sampled ranks (empty = all of the stride)
+    long long items = 0;               // subgraphs to process
+    bool inplace = false;              // k == 0
+    bool empty = false;                // nothing to fit
+    bool batchable = false;
+    std::vector<int> ioff, pairs;      // common-neighbour pairs (parent numbering)
+    int M = 0;
+    double *ms_host = nullptr;         // multiset matrix (caller owns after return)
+    std::vector<long long> values_host;  // per-subgraph path: values collected on the host
+    std::vector<long long> hist;       // flat [bits, count]
+    unsigned long long sweeps = 0, edge_iters = 0, fits = 0;
+};
+
+Status prepare(Prep &p)
+{
+    dressx_hist_request_t *r = p.r;
+    p_dress_graph_t g = r->graph;
+    if (!g) return Status::Err(DRESSX_EINVAL, "request without graph");
+    if (r->kind != DRESSX_DELTA && r->kind != DRESSX_NABLA) return Status::Err(DRESSX_EINVAL, "bad request kind");
+    if (r->stride < 1 || r->offset < 0) return Status::Err(DRESSX_EINVAL, "bad offset/stride");
+    p.g = g;
+    p.N = g->N;
+    p.E = g->E;
+    p.S = g->N > 0 ? g->adj_offset[g->N] : 0;
+    const int k = r->k;
+    p.total = k == 0 ? 1 : (r->kind == DRESSX_DELTA ? binom_h(p.N, k) : perm_h(p.N, k));
+    r->num_subgraphs = p.total;
+    const bool want_ms = r->keep_multisets != 0;
+    // matrices beyond 2^31 entries are not allocated (the caller gets NULL,
+    // as when the reference's malloc fails)
+    if (want_ms && p.total >= 0 && (p.E == 0 || p.total <= (1LL << 31) / p.E)) {
+        size_t len = (size_t)p.total * (size_t)p.E;
+        p.ms_host = (double *)std::malloc((len ? len : 1) * sizeof(double));
+        if (p.ms_host)
+            for (size_t i = 0; i < len; ++i) p.ms_host[i] = std::nan("");
+    }
+    if (k == 0) {
+        p.inplace = r->offset == 0;
+        p.empty = !p.inplace;
+        return Status::Ok();
+    }
+    if (k < 0 || k >= p.N) {
+        p.empty = true;
+        return Status::Ok();
+    }
+    p.per = (p.total + r->stride - 1 - r->offset) / r->stride;
+    if (p.per < 0) p.per = 0;
+    if (r->n_samples > 0 && r->n_samples < p.per) {
+        std::vector<long long> picks = sample_picks(p.per, r->n_samples, r->seed, r->offset);
+        p.ranks.resize(picks.size());
+        for (size_t i = 0; i < picks.size(); ++i) p.ranks[i] = r->offset + picks[i] * (long long)r->stride;
+        p.items = (long long)picks.size();
+    } else {
+        p.items = p.per;
+    }
+    if (p.items == 0) {
+        p.empty = true;
+        return Status::Ok();
+    }
+
+    // common-neighbour pairs of the parent by the reference's merge walk
+    // (libdress/src/dress.c:307-363); masks filter them per subgraph
+    const int *off = g->adj_offset, *tg = g->adj_target, *ei = g->adj_edge_idx;
+    int maxdeg = 0;
+    bool dup = false;
+    for (int u = 0; u < p.N; ++u) {
+        maxdeg = std::max(maxdeg, off[u + 1] - off[u]);
+        for (int s = off[u] + 1; s < off[u + 1]; ++s) dup |= tg[s] == tg[s - 1];
+    }
+    p.ioff.assign((size_t)p.E + 1, 0);
+    for (int e = 0; e < p.E; ++e) {
+        int iu = off[g->U[e]], iu_end = off[g->U[e] + 1];
+        int iv = off[g->V[e]], iv_end = off[g->V[e] + 1];
+        while (iu < iu_end && iv < iv_end) {
+            int x = tg[iu], y = tg[iv];
+            if (x == y) { p.pairs.push_back(ei[iu]); p.pairs.push_back(ei[iv]); }
+            iu += (x <= y);
+            iv += (x >= y);
+        }
+        p.ioff[(size_t)e + 1] = (int)(p.pairs.size() / 2);
+    }
+    p.T = p.ioff[(size_t)p.E];
+    p.M = std::max(2, next_pow2(maxdeg + 1));
+    // Masks reproduce the rebuilt subgraph except for the reciprocal-weight
+    // lookup of DIRECTED graphs with repeated directed edges.
+    p.batchable = p.M <= 32 && !(dup && g->variant == DRESS_VARIANT_DIRECTED);
+    return Status::Ok();
+}
+
+// ---- per-subgraph path ----------------------------------------------------------
+Status run_per_fit(Prep &p)
+{
+    dressx_hist_request_t *r = p.r;
+    p_dress_graph_t g = p.g;
+    const int N = p.N, E = p.E, k = r->k;
+    std::vector<int> sel((size_t)k);
+    std::vector<int> vmap((size_t)N);
+    auto process = [&](long long s) -> Status {
+        // unrank s
+        if (r->kind == DRESSX_DELTA) {
+            long long rr = s;
+            int c = 0;
+            for (int i = 0; i < k; ++i) {
+                for (;;) {
+                    long long cnt = binom_h(N - c - 1, k - i - 1);
+                    if (rr < cnt) break;
+                    rr -= cnt;
+                    ++c;
+                }
+                sel[(size_t)i] = c++;
+            }
+        } else {
+            long long rr = s;
+            for (int i = 0; i < k; ++i) {
+                long long per = perm_h(N - i - 1, k - i - 1);
+                long long idx = rr / per;
+                rr -= idx * per;
+                int v = 0, seen = -1;
+                for (;; ++v) {
+                    bool used = false;
+                    for (int j = 0; j < i; ++j) used |= sel[(size_t)j] == v;
+                    if (!used && ++seen == idx) break;
+                }
+                sel[(size_t)i] = v;
+            }
+        }
+        // build the subgraph (libdress/src/delta_dress_impl.c:33-107,
+        // nabla_dress_impl.c:61-91)
+        int sN = N, sE = 0;
+        int *sU, *sV;
+        double *sW = nullptr, *sNW = nullptr;
+        std::vector<int> emap((size_t)E, -1);
+        if (r->kind == DRESSX_DELTA) {
+            int nid = 0;
+            for (int v = 0; v < N; ++v) {
+                bool del = false;
+                for (int i = 0; i < k; ++i) del |= sel[(size_t)i] == v;
+                vmap[(size_t)v] = del ? -1 : nid++;
+            }
+            sN = N - k;
+            for (int e = 0; e < E; ++e) sE += vmap[(size_t)g->U[e]] >= 0 && vmap[(size_t)g->V[e]] >= 0;
+            if (sE == 0) return Status::Ok();
+            sU = (int *)std::malloc((size_t)sE * sizeof(int));
+            sV = (int *)std::malloc((size_t)sE * sizeof(int));
+            if (g->W) sW = (double *)std::malloc((size_t)sE * sizeof(double));
+            for (int e = 0, j = 0; e < E; ++e) {
+                int a = vmap[(size_t)g->U[e]], b = vmap[(size_t)g->V[e]];
+                if (a >= 0 && b >= 0) {
+                    sU[j] = a; sV[j] = b;
+                    if (sW) sW[j] = g->W[e];
+                    emap[(size_t)e] = j++;
+                }
+            }
+        } else {
+            sE = E;
+            sU = (int *)std::malloc((size_t)(E ? E : 1) * sizeof(int));
+            sV = (int *)std::malloc((size_t)(E ? E : 1) * sizeof(int));
+            std::memcpy(sU, g->U, (size_t)E * sizeof(int));
+            std::memcpy(sV, g->V, (size_t)E * sizeof(int));
+            if (g->W) {
+                sW = (double *)std::malloc((size_t)(E ? E : 1) * sizeof(double));
+                std::memcpy(sW, g->W, (size_t)E * sizeof(double));
+            }
+            sNW = (double *)std::malloc((size_t)(N ? N : 1) * sizeof(double));
+            for (int v = 0; v < N; ++v) sNW[v] = 1.0;
+            static const int pr[16] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53};
+            for (int i = 0; i < k; ++i)
+                sNW[sel[(size_t)i]] = std::sqrt((double)(i < 16 ? pr[i] : 2 * i + 3));
+            for (int e = 0; e < E; ++e) emap[(size_t)e] = e;
+        }
+        p_dress_graph_t sub = dress_init_graph(sN, sE, sU, sV, sW, sNW, g->variant, g->precompute_intercepts);
+        if (!sub) return Status::Err(DRESSX_EINVAL, "subgraph construction failed");
+        FitStats fs;
+        Status st = fit_graph(sub, r->max_iterations, r->epsilon, nullptr, nullptr, &fs);
+        if (!st.ok()) {
+            dress_free_graph(sub);
+            return st;
+        }
+        for (int e = 0; e < sub->E; ++e) {
+            long long b;
+            std::memcpy(&b, &sub->edge_dress[e], sizeof(b));
+            p.values_host.push_back(b);
+        }
+        if (p.ms_host)
+            for (int e = 0; e < E; ++e)
+                p.ms_host[(size_t)s * E + e] = emap[(size_t)e] >= 0 ? sub->edge_dress[emap[(size_t)e]] : std::nan("");
+        p.sweeps += (unsigned long long)fs.sweeps;
+        p.edge_iters += (unsigned long long)fs.sweeps * (unsigned long long)sub->E;
+        p.fits += 1;
+        dress_free_graph(sub);
+        return Status::Ok();
+    };
+    for (long long i = 0; i < p.items; ++i) {
+        long long s = p.ranks.empty() ? r->offset + i * (long long)r->stride : p.ranks[(size_t)i];
+        DRESS_TRY(process(s));
+    }
+    return Status::Ok();
+}
+
+// ---- histogram of host-collected values (in-place fits, per-subgraph path) -------
+Status hist_of_host_values(std::vector<Prep *> &ps, cudaStream_t st, int sms)
+{
+    long long total = 0;
+    for (Prep *p : ps) total += (long long)p->values_host.size();
+    if (total == 0) return Status::Ok();
+    DevBuf<unsigned long long> keys, alt;
+    DRESS_TRY(keys.alloc((size_t)total, st));
+    DRESS_TRY(alt.alloc((size_t)total, st));
+    std::vector<long long> begin, len;
+    long long o = 0;
+    for (Prep *p : ps) {
+        begin.push_back(o);
+        len.push_back((long long)p->values_host.size());
+        if (!p->values_host.empty())
+            DRESS_CUDA_TRY(cudaMemcpyAsync(keys.get() + o, p->values_host.data(),
+                                           p->values_host.size() * sizeof(long long), cudaMemcpyHostToDevice, st));
+        o += (long long)p->values_host.size();
+    }
+    std::vector<std::vector<long long>> out;
+    DRESS_TRY(histogram_segments(keys.get(), alt.get(), begin, len, out, st, sms));
+    for (size_t i = 0; i < ps.size(); ++i) ps[i]->hist = std::move(out[i]);
+    return Status::Ok();
+}
+
+// ---- batched path ------------------------------------------------------------------
+struct Tune {
+    int gsize, groups;
+};
+
+// Threads per subgraph by edge count (sweeps of a few hundred edges keep a
+// warp busy; larger subgraphs split across more warps).
+Tune pick_tune(int maxE, int maxN, int M, const dressx_config_t &cfg)
+{
+    int gs = cfg.group_threads > 0 ? cfg.group_threads
+           : maxE <= 640 ? 32 : maxE <= 2048 ? 64 : maxE <= 8192 ? 128 : 256;
+    (void)maxN;
+    (void)M;
+    int groups = 512 / gs;
+    if (gs > 32 && groups > 15) groups = 15;
+    return {gs, groups};
+}
+
+Status run_batched(std::vector<Prep *> &ps, Engine &en)
+{
+    cudaStream_t st = en.stream;
+    int smem_optin = 0;
+    DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, en.device));
+    const long long smem_cap = smem_optin - 256;
+
+    // one launch for all batchable requests
+    int maxE = 1, maxN = 1, maxk = 1, M = 2;
+    long long maxbytes = 16, arena = 0, values = 0, ms_total = 0, nranks = 0;
+    std::vector<ParentDesc> descs;
+    std::vector<long long> val_base;
+    for (Prep *p : ps) {
+        ParentLayout PL = parent_layout(p->N, p->E, p->S, p->T, 0, 0);
+        maxE = std::max(maxE, p->E);
+        maxN = std::max(maxN, p->N);
+        maxk = std::max(maxk, p->r->k);
+        M = std::max(M, p->M);
+        maxbytes = std::max(maxbytes, PL.bytes);
+        ParentDesc d{};
+        d.N = p->N; d.E = p->E; d.S = p->S; d.T = p->T;
+        d.kind = p->r->kind == DRESSX_DELTA ? ITEM_DELTA : ITEM_NABLA;
+        d.k = p->r->k;
+        d.fwd = p->g->variant == DRESS_VARIANT_FORWARD || p->g->variant == DRESS_VARIANT_BACKWARD;
+        d.max_iter = p->r->max_iterations;
+        d.eps = p->r->epsilon;
+        d.req = (int)descs.size();
+        d.data_off = arena;
+        d.offset = p->r->offset;
+        d.stride = p->r->stride;
+        d.ranks_off = p->ranks.empty() ? -1 : nranks;
+        d.val_base = values;
+        d.ms_base = p->ms_host ? ms_total : -1;
+        d.E_ms = p->E;
+        descs.push_back(d);
+        val_base.push_back(values);
+        arena += PL.bytes;
+        values += p->items * (long long)p->E;
+        nranks += (long long)p->ranks.size();
+        if (p->ms_host) ms_total += p->total * (long long)p->E;
+    }
+    Tune tu = pick_tune(maxE, maxN, M, en.cfg);
+    BatchLaunch L{};
+    L.gsize = tu.gsize;
+    L.maxE = maxE;
+    L.maxN = maxN;
+    L.maxk = maxk;
+    L.M = M;
+    L.parent_bytes = maxbytes;
+    // shrink the group count until parent + group states fit; drop staging last
+    L.stage = 1;
+    L.groups = tu.groups;
+    while (L.groups > 1 && (long long)batch_smem_bytes(L) > smem_cap) --L.groups;
+    if ((long long)batch_smem_bytes(L) > smem_cap) {
+        L.stage = 0;
+        L.groups = tu.groups;
+        while (L.groups > 1 && (long long)batch_smem_bytes(L) > smem_cap) --L.groups;
+    }
+    if ((long long)batch_smem_bytes(L) > smem_cap)
+        return Status::Err(DRESSX_EUNSUPPORTED, "subgraph state exceeds shared memory");
+    if (L.stage && L.groups * 2 < tu.groups) {
+        // staging leaves too few groups: read parents from L2 instead
+        BatchLaunch L2 = L;
+        L2.stage = 0;
+        L2.groups = tu.groups;
+        while (L2.groups > 1 && (long long)batch_smem_bytes(L2) > smem_cap) --L2.groups;
+        if (L2.groups > L.groups) L = L2;
+    }
+
+    // pack parents
+    std::vector<unsigned char> hbytes((size_t)arena);
+    std::vector<long long> hranks;
+    hranks.reserve((size_t)nranks);
+    for (size_t i = 0; i < ps.size(); ++i) {
+        Prep *p = ps[i];
+        p_dress_graph_t g = p->g;
+        ParentLayout PL = parent_layout(p->N, p->E, p->S, p->T, 0, 0);
+        unsigned char *b = hbytes.data() + descs[i].data_off;
+        std::memcpy(b + PL.U, g->U, (size_t)p->E * 4);
+        std::memcpy(b + PL.V, g->V, (size_t)p->E * 4);
+        std::memcpy(b + PL.w, g->edge_weight, (size_t)p->E * 8);
+        std::memcpy(b + PL.row_off, g->adj_offset, (size_t)(p->N + 1) * 4);
+        std::memcpy(b + PL.row_eid, g->adj_edge_idx, (size_t)p->S * 4);
+        std::memcpy(b + PL.ioff, p->ioff.data(), (size_t)(p->E + 1) * 4);
+        if (p->T) std::memcpy(b + PL.pairs, p->pairs.data(), (size_t)p->T * 8);
+        hranks.insert(hranks.end(), p->ranks.begin(), p->ranks.end());
+    }
+    // chunks: a few rounds of subgraphs per CTA visit
+    std::vector<Chunk> chunks;
+    const int chunk_items = 4 * L.groups;
+    for (size_t i = 0; i < ps.size(); ++i)
+        for (long long f = 0; f < ps[i]->items; f += chunk_items)
+            chunks.push_back({(int)i, (int)std::min<long long>(chunk_items, ps[i]->items - f), f});
+
+    const int nreq = (int)ps.size();
+    DevBuf<unsigned char> d_pdata;
+    DevBuf<ParentDesc> d_desc;
+    DevBuf<Chunk> d_chunks;
+    DevBuf<long long> d_ranks;
+    DevBuf<unsigned long long> d_vals, d_alt, d_stats;
+    DevBuf<double> d_ms;
+    DevBuf<int> d_counter;
+    DRESS_TRY(d_pdata.alloc((size_t)arena, st));
+    DRESS_TRY(d_desc.alloc(descs.size(), st));
+    DRESS_TRY(d_chunks.alloc(chunks.size(), st));
+    DRESS_TRY(d_ranks.alloc(hranks.size() + 1, st));
+    DRESS_TRY(d_vals.alloc((size_t)values + 1, st));
+    DRESS_TRY(d_stats.alloc(4 * (size_t)nreq, st));
+    DRESS_TRY(d_counter.alloc(1, st));
+    if (ms_total > 0) DRESS_TRY(d_ms.alloc((size_t)ms_total, st));
+    DRESS_CUDA_TRY(cudaMemcpyAsync(d_pdata.get(), hbytes.data(), (size_t)arena, cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(cudaMemcpyAsync(d_desc.get(), descs.data(), descs.size() * sizeof(ParentDesc),
+                                   cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(cudaMemcpyAsync(d_chunks.get(), chunks.data(), chunks.size() * sizeof(Chunk),
+                                   cudaMemcpyHostToDevice, st));
+    if (!hranks.empty())
+        DRESS_CUDA_TRY(cudaMemcpyAsync(d_ranks.get(), hranks.data(), hranks.size() * sizeof(long long),
+                                       cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_stats.get(), 0, 4 * (size_t)nreq * sizeof(unsigned long long), st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_counter.get(), 0, sizeof(int), st));
+    if (ms_total > 0) {
+        // the rows of unprocessed subgraphs stay NaN, as in the reference
+        size_t o = 0;
+        for (Prep *p : ps)
+            if (p->ms_host) {
+                size_t len = (size_t)p->total * (size_t)p->E;
+                DRESS_CUDA_TRY(cudaMemcpyAsync(d_ms.get() + o, p->ms_host, len * sizeof(double),
+                                               cudaMemcpyHostToDevice, st));
+                o += len;
+            }
+    }
+    L.parents = d_desc.get();
+    L.pdata = d_pdata.get();
+    L.chunks = d_chunks.get();
+    L.nchunks = (int)chunks.size();
+    L.chunk_counter = d_counter.get();
+    L.ranks = d_ranks.get();
+    L.values = (double *)d_vals.get();
+    L.cursors = d_stats.get();
+    L.sweeps = d_stats.get() + nreq;
+    L.edge_iters = d_stats.get() + 2 * nreq;
+    L.fits = d_stats.get() + 3 * nreq;
+    L.multisets = d_ms.get();
+    DRESS_TRY(launch_batch(L, en.num_sms, st));
+
+    std::vector<unsigned long long> stats(4 * (size_t)nreq);
+    DRESS_CUDA_TRY(cudaMemcpyAsync(stats.data(), d_stats.get(), stats.size() * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<long long> begin((size_t)nreq), len((size_t)nreq);
+    for (int i = 0; i < nreq; ++i) {
+        begin[(size_t)i] = val_base[(size_t)i];
+        len[(size_t)i] = (long long)stats[(size_t)i];
+        ps[(size_t)i]->sweeps += stats[(size_t)nreq + i];
+        ps[(size_t)i]->edge_iters += stats[2 * (size_t)nreq + i];
+        ps[(size_t)i]->fits += stats[3 * (size_t)nreq + i];
+    }
+    bool need_hist = false;
+    for (Prep *p : ps) need_hist |= p->r->want_histogram != 0;
+    if (need_hist) {
+        DRESS_TRY(d_alt.alloc((size_t)values + 1, st));
+        std::vector<std::vector<long long>> out;
+        DRESS_TRY(histogram_segments(d_vals.get(), d_alt.get(), begin, len, out, st, en.num_sms));
+        for (int i = 0; i < nreq; ++i) ps[(size_t)i]->hist = std::move(out[(size_t)i]);
+    }
+    if (ms_total > 0) {
+        size_t o = 0;
+        for (Prep *p : ps)
+            if (p->ms_host) {
+                size_t n = (size_t)p->total * (size_t)p->E;
+                DRESS_CUDA_TRY(cudaMemcpyAsync(p->ms_host, d_ms.get() + o, n * sizeof(double),
+                                               cudaMemcpyDeviceToHost, st));
+                o += n;
+            }
+        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return Status::Ok();
+}
+
+Status finish(Prep &p)
+{
+    dressx_hist_request_t *r = p.r;
+    r->fits = (int64_t)p.fits;
+    r->hist_flat = nullptr;
+    r->hist_len = 0;
+    if (r->want_histogram && !p.hist.empty()) {
+        r->hist_flat = (int64_t *)std::malloc(p.hist.size() * sizeof(int64_t));
+        if (!r->hist_flat) return Status::Err(DRESSX_ENOMEM, "host allocation of the histogram failed");
+        std::memcpy(r->hist_flat, p.hist.data(), p.hist.size() * sizeof(int64_t));
+        r->hist_len = (int)p.hist.size();
+    }
+    r->multisets = p.ms_host;
+    p.ms_host = nullptr;
+    return Status::Ok();
+}
+
+Status hist_batch_impl(dressx_hist_request_t *reqs, int n, bool per_fit)
+{
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    DRESS_TRY(en.init());
+    DRESS_CUDA_TRY(cudaSetDevice(en.device));
+    std::vector<Prep> ps((size_t)n);
+    Status first;
+    for (int i = 0; i < n; ++i) {
+        ps[(size_t)i].r = &reqs[i];
+        reqs[i].status = DRESSX_OK;
+        reqs[i].hist_flat = nullptr;
+        reqs[i].hist_len = 0;
+        reqs[i].multisets = nullptr;
+        reqs[i].fits = 0;
+        Status s = prepare(ps[(size_t)i]);
+        if (!s.ok()) {
+            reqs[i].status = s.code;
+            if (first.ok()) first = s;
+        }
+    }
+    std::vector<Prep *> batch, host_vals;
+    for (auto &p : ps) {
+        if (p.r->status != DRESSX_OK || p.empty) continue;
+        if (p.inplace) {
+            // k == 0: fit the caller's graph itself (libdress/src/delta_dress_impl.c:206-224)
+            FitStats fs;
+            Status s = fit_graph(p.g, p.r->max_iterations, p.r->epsilon, nullptr, nullptr, &fs);
+            if (!s.ok()) { p.r->status = s.code; if (first.ok()) first = s; continue; }
+            for (int e = 0; e < p.E; ++e) {
+                long long b;
+                std::memcpy(&b, &p.g->edge_dress[e], sizeof(b));
+                p.values_host.push_back(b);
+                if (p.ms_host) p.ms_host[e] = p.g->edge_dress[e];
+            }
+            p.fits = 1;
+            p.sweeps = (unsigned long long)fs.sweeps;
+            p.edge_iters = (unsigned long long)fs.sweeps * (unsigned long long)p.E;
+            host_vals.push_back(&p);
+        } else if (p.batchable && !per_fit) {
+            batch.push_back(&p);
+        } else {
+            Status s = run_per_fit(p);
+            if (!s.ok()) { p.r->status = s.code; if (first.ok()) first = s; continue; }
+            host_vals.push_back(&p);
+        }
+    }
+    if (!batch.empty()) {
+        Status s = run_batched(batch, en);
+        if (!s.ok()) {
+            for (Prep *p : batch) p->r->status = s.code;
+            if (first.ok()) first = s;
+        }
+    }
+    {
+        std::vector<Prep *> hv;
+        for (Prep *p : host_vals)
+            if (p->r->want_histogram) hv.push_back(p);
+        Status s = hist_of_host_values(hv, en.stream, en.num_sms);
+        if (!s.ok()) {
+            for (Prep *p : hv) p->r->status = s.code;
+            if (first.ok()) first = s;
+        }
+    }
+    for (auto &p : ps) {
+        if (p.r->status == DRESSX_OK) {
+            Status s = finish(p);
+            if (!s.ok()) { p.r->status = s.code; if (first.ok()) first = s; }
+        }
+        if (p.ms_host) { std::free(p.ms_host); p.ms_host = nullptr; }
+    }
+    return first;
+}
+
+// ---- legacy wrappers -------------------------------------------------------------------
+int64_t *legacy_flat(int kind, p_dress_graph_t g, int k, int iterations, double epsilon, int n_samples,
+                     unsigned int seed, int *hist_size, int keep_multisets, double **multisets,
+                     int64_t *num, int offset, int stride)
+{
+    dressx_hist_request_t r{};
+    r.graph = g;
+    r.kind = kind;
+    r.k = k;
+    r.max_iterations = iterations;
+    r.epsilon = epsilon;
+    r.n_samples = n_samples;
+    r.seed = seed;
+    r.offset = offset;
+    r.stride = stride;
+    r.want_histogram = hist_size != nullptr;
+    r.keep_multisets = keep_multisets && multisets;
+    Status s = hist_batch_impl(&r, 1, false);
+    set_last_error(s);
+    if (hist_size) *hist_size = 0;
+    if (!s.ok()) return nullptr;
+    if (num) *num = r.num_subgraphs;
+    if (keep_multisets && multisets) *multisets = r.multisets;
+    if (hist_size) *hist_size = r.hist_len;
+    return r.hist_flat;
+}
+
+dress_hist_pair_t *flat_to_pairs(int64_t *flat, int flat_len, int *hist_size)
+{
+    int n = flat_len / 2;
+    if (hist_size) *hist_size = n;
+    if (!flat || n <= 0) {
+        std::free(flat);
+        return nullptr;
+    }
+    dress_hist_pair_t *pairs = (dress_hist_pair_t *)std::malloc((size_t)n * sizeof(dress_hist_pair_t));
+    if (pairs)
+        for (int i = 0; i < n; ++i) {
+            std::memcpy(&pairs[i].value, &flat[2 * i], sizeof(double));
+            pairs[i].count = flat[2 * i + 1];
+        }
+    std::free(flat);
+    return pairs;
+}
+
+}  // namespace
+}  // namespace dress
+
+using namespace dress;
+
+extern "C" {
+
+int dressx_hist_batch(dressx_hist_request_t *reqs, int n)
+{
+    if (!reqs || n < 0) return DRESSX_EINVAL;
+    Status s = hist_batch_impl(reqs, n, false);
+    set_last_error(s);
+    return s.code;
+}
+
+int dressx_hist_batch_per_fit(dressx_hist_request_t *reqs, int n)
+{
+    if (!reqs || n < 0) return DRESSX_EINVAL;
+    Status s = hist_batch_impl(reqs, n, true);
+    set_last_error(s);
+    return s.code;
+}
+
+int64_t *dress_delta_fit_cuda_strided_flat(p_dress_graph_t g, int k, int iterations, double epsilon, int n_samples,
+                                           unsigned int seed, int *hist_size, int keep_multisets,
+                                           double **multisets, int64_t *num_subgraphs, int offset, int stride)
+{
+    return legacy_flat(DRESSX_DELTA, g, k, iterations, epsilon, n_samples, seed, hist_size, keep_multisets,
+                       multisets, num_subgraphs, offset, stride);
+}
+
+int64_t *dress_delta_fit_cuda_flat(p_dress_graph_t g, int k, int iterations, double epsilon, int n_samples,
+                                   unsigned int seed, int *hist_size, int keep_multisets, double **multisets,
+                                   int64_t *num_subgraphs)
+{
+    return legacy_flat(DRESSX_DELTA, g, k, iterations, epsilon, n_samples, seed, hist_size, keep_multisets,
+                       multisets, num_subgraphs, 0, 1);
+}
+
+dress_hist_pair_t *dress_delta_fit_cuda_strided(p_dress_graph_t g, int k, int iterations, double epsilon,
+                                                int n_samples, unsigned int seed, int *hist_size,
+                                                int keep_multisets, double **multisets, int64_t *num_subgraphs,
+                                                int offset, int stride)
+{
+    int flat_len = 0;
+    int64_t *flat = legacy_flat(DRESSX_DELTA, g, k, iterations, epsilon, n_samples, seed,
+                                hist_size ? &flat_len : nullptr, keep_multisets, multisets, num_subgraphs,
+                                offset, stride);
+    return flat_to_pairs(flat, flat_len, hist_size);
+}
+
+dress_hist_pair_t *dress_delta_fit_cuda(p_dress_graph_t g, int k, int iterations, double epsilon, int n_samples,
+                                        unsigned int seed, int *hist_size, int keep_multisets,
+                                        double **multisets, int64_t *num_subgraphs)
+{
+    return dress_delta_fit_cuda_strided(g, k, iterations, epsilon, n_samples, seed, hist_size, keep_multisets,
+                                        multisets, num_subgraphs, 0, 1);
+}
+
+int64_t *dress_nabla_fit_cuda_strided_flat(p_dress_graph_t g, int k, int iterations, double epsilon, int n_samples,
+                                           unsigned int seed, int *hist_size, int keep_multisets,
+                                           double **multisets, int64_t *num_tuples, int offset, int stride)
+{
+    return legacy_flat(DRESSX_NABLA, g, k, iterations, epsilon, n_samples, seed, hist_size, keep_multisets,
+                       multisets, num_tuples, offset, stride);
+}
+
+int64_t *dress_nabla_fit_cuda_flat(p_dress_graph_t g, int k, int iterations, double epsilon, int n_samples,
+                                   unsigned int seed, int *hist_size, int keep_multisets, double **multisets,
+                                   int64_t *num_tuples)
+{
+    return legacy_flat(DRESSX_NABLA, g, k, iterations, epsilon, n_samples, seed, hist_size, keep_multisets,
+                       multisets, num_tuples, 0, 1);
+}
+
+dress_hist_pair_t *dress_nabla_fit_cuda_strided(p_dress_graph_t g, int k, int iterations, double epsilon,
+                                                int n_samples, unsigned int seed, int *hist_size,
+                                                int keep_multisets, double **multisets, int64_t *num_tuples,
+                                                int offset, int stride)
+{
+    int flat_len = 0;
+    int64_t *flat = legacy_flat(DRESSX_NABLA, g, k, iterations, epsilon, n_samples, seed,
+                                hist_size ? &flat_len : nullptr, keep_multisets, multisets, num_tuples, offset,
+                                stride);
+    return flat_to_pairs(flat, flat_len, hist_size);
+}
+
+dress_hist_pair_t *dress_nabla_fit_cuda(p_dress_graph_t g, int k, int iterations, double epsilon, int n_samples,
+                                        unsigned int seed, int *hist_size, int keep_multisets,
+                                        double **multisets, int64_t *num_tuples)
+{
+    return dress_nabla_fit_cuda_strided(g, k, iterations, epsilon, n_samples, seed, hist_size, keep_multisets,
+                                        multisets, num_tuples, 0, 1);
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// engine.cpp -- process-wide engine state and the fit entry points.
+//
+// One engine per process: a non-blocking stream on the device that was
+// current at first use (or dressx_config_t.device), a side stream, and the
+// device's default memory pool with a high release threshold so buffers are
+// recycled between calls instead of returned to the driver.  Legacy entry
+// points are serialised by a mutex; none of them calls exit().
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "engine.h"
+
+namespace dress {
+
+namespace {
+std::mutex g_err_mu;
+int g_err_code = DRESSX_OK;
+std::string g_err_msg;
+FitStats g_last_stats;
+}  // namespace
+
+void set_last_error(const Status &s)
+{
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err_code = s.code;
+    g_err_msg = s.msg;
+    if (!s.ok()) std::fprintf(stderr, "dress_b200: %s\n", s.msg.c_str());
+}
+
+Pinned::~Pinned()
+{
+    if (base_) cudaFreeHost(base_);
+}
+
+Status Pinned::reserve(size_t bytes)
+{
+    if (bytes <= cap_) return Status::Ok();
+    if (base_) cudaFreeHost(base_);
+    base_ = nullptr;
+    cap_ = 0;
+    if (cudaMallocHost((void **)&base_, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        base_ = nullptr;
+        return Status::Err(DRESSX_ENOMEM, "pinned host allocation failed");
+    }
+    cap_ = bytes;
+    return Status::Ok();
+}
+
+Status Engine::init()
+{
+    if (stream) return Status::Ok();
+    int dev = cfg.device;
+    if (dev < 0) DRESS_CUDA_TRY(cudaGetDevice(&dev));
+    DRESS_CUDA_TRY(cudaSetDevice(dev));
+    device = dev;
+    DRESS_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+    DRESS_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DRESS_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    DRESS_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    cudaMemPool_t pool;
+    DRESS_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+    unsigned long long keep = cfg.memory_budget_bytes ? cfg.memory_budget_bytes : ~0ULL;
+    DRESS_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    return Status::Ok();
+}
+
+Engine &engine()
+{
+    static Engine e;
+    return e;
+}
+
+Status fit_locked(p_dress_graph_t g, int max_iterations, double epsilon, int *iterations, double *delta)
+{
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    DRESS_TRY(en.init());
+    DRESS_CUDA_TRY(cudaSetDevice(en.device));
+    FitStats st;
+    Status s = fit_graph(g, max_iterations, epsilon, iterations, delta, &st);
+    if (s.ok()) g_last_stats = st;
+    return s;
+}
+
+}  // namespace dress
+
+using namespace dress;
+
+extern "C" {
+
+int dressx_configure(const dressx_config_t *cfg)
+{
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    if (!cfg) return DRESSX_EINVAL;
+    if (en.stream && cfg->device >= 0 && cfg->device != en.device) {
+        set_last_error(Status::Err(DRESSX_EINVAL, "engine already bound to another device"));
+        return DRESSX_EINVAL;
+    }
+    en.cfg = *cfg;
+    return DRESSX_OK;
+}
+
+int dressx_last_error(char *msg, int msg_len)
+{
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    if (msg && msg_len > 0) {
+        std::strncpy(msg, g_err_msg.c_str(), (size_t)msg_len - 1);
+        msg[msg_len - 1] = 0;
+    }
+    return g_err_code;
+}
+
+int dressx_fit(p_dress_graph_t g, int max_iterations, double epsilon, int *iterations, double *delta)
+{
+    Status s = fit_locked(g, max_iterations, epsilon, iterations, delta);
+    set_last_error(s);
+    return s.code;
+}
+
+int dressx_last_fit_stats(dressx_fit_stats_t *out)
+{
+    if (!out) return DRESSX_EINVAL;
+    out->common_terms = g_last_stats.T;
+    out->sweeps = g_last_stats.sweeps;
+    out->setup_ms = g_last_stats.setup_ms;
+    out->iterate_ms = g_last_stats.iterate_ms;
+    return DRESSX_OK;
+}
+
+void dress_fit_cuda(p_dress_graph_t g, int max_iterations, double epsilon, int *iterations, double *delta)
+{
+    dressx_fit(g, max_iterations, epsilon, iterations, delta);
+}
+
+void dress_fit(p_dress_graph_t g, int max_iterations, double epsilon, int *iterations, double *delta)
+{
+    dressx_fit(g, max_iterations, epsilon, iterations, delta);
+}
+
+void dressx_free(void *p) { free(p); }
+
+}  // extern "C"

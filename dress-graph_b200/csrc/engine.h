@@ -1,0 +1,122 @@
+// engine.h -- internal C++ interface of the B200 DRESS engine.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dress_b200.h"
+#include "dress_b200_ext.h"
+
+namespace dress {
+
+// ---- status ------------------------------------------------------------
+struct Status {
+    int code = DRESSX_OK;
+    std::string msg;
+    bool ok() const { return code == DRESSX_OK; }
+    static Status Ok() { return Status(); }
+    static Status Err(int c, const std::string &m) { Status s; s.code = c; s.msg = m; return s; }
+};
+
+#define DRESS_CUDA_TRY(call)                                                   \
+    do {                                                                       \
+        cudaError_t _e = (call);                                               \
+        if (_e != cudaSuccess)                                                 \
+            return ::dress::Status::Err(DRESSX_ECUDA,                          \
+                std::string(#call) + ": " + cudaGetErrorString(_e));           \
+    } while (0)
+
+#define DRESS_TRY(expr)                                                        \
+    do {                                                                       \
+        ::dress::Status _s = (expr);                                           \
+        if (!_s.ok()) return _s;                                               \
+    } while (0)
+
+// ---- stream-ordered device buffers -------------------------------------
+// Device memory comes from the device's default memory pool through
+// cudaMallocAsync on the engine stream.  The pool keeps freed blocks
+// (release threshold = the configured budget), so repeated calls of the same
+// size allocate nothing from the driver after the first one.
+template <class T>
+class DevBuf {
+  public:
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    Status alloc(size_t n, cudaStream_t st)
+    {
+        release();
+        st_ = st;
+        n_ = n;
+        if (n == 0) return Status::Ok();
+        cudaError_t e = cudaMallocAsync((void **)&p_, n * sizeof(T), st);
+        if (e != cudaSuccess) {
+            p_ = nullptr;
+            cudaGetLastError();
+            return Status::Err(DRESSX_ENOMEM, "device allocation of " +
+                               std::to_string(n * sizeof(T)) + " bytes failed");
+        }
+        return Status::Ok();
+    }
+    void release()
+    {
+        if (p_) cudaFreeAsync(p_, st_);
+        p_ = nullptr;
+        n_ = 0;
+    }
+    T *get() const { return p_; }
+    size_t size() const { return n_; }
+  private:
+    T *p_ = nullptr;
+    size_t n_ = 0;
+    cudaStream_t st_ = nullptr;
+};
+
+// ---- pinned host staging buffer ------------------------------------------
+class Pinned {
+  public:
+    ~Pinned();
+    Status reserve(size_t bytes);
+    char *ptr() { return base_; }
+  private:
+    char *base_ = nullptr;
+    size_t cap_ = 0;
+};
+
+// ---- the per-process engine ------------------------------------------------
+struct Engine {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;           // second stream for overlapped bins
+    cudaEvent_t fork = nullptr, join = nullptr;
+    std::mutex mu;                         // legacy entry points are serialised
+    Pinned pinned;
+    int num_sms = 148;
+    dressx_config_t cfg;
+    Status init();
+};
+
+Engine &engine();
+void set_last_error(const Status &s);
+
+// ---- device utilities (scan.cu) -------------------------------------------
+// out[i] = sum_{j<i} in[i] for i in [0, n], out[n] = total.  `tmp` must hold
+// scan_tmp_elems(n) int64 values.
+size_t scan_tmp_elems(long long n);
+Status exclusive_scan_i32(const int *in, long long *out, long long n, long long *tmp, cudaStream_t st);
+Status exclusive_scan_i64(const long long *in, long long *out, long long n, long long *tmp, cudaStream_t st);
+
+// ---- single-graph fit (fit_graph.cu) --------------------------------------
+struct FitStats {
+    long long T = 0;            // common-neighbour terms per sweep
+    int sweeps = 0;             // sweeps executed
+    double setup_ms = 0, iterate_ms = 0;
+};
+Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon,
+                 int *iterations, double *delta, FitStats *stats);
+
+}  // namespace dress

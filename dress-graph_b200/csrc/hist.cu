@@ -1,0 +1,313 @@
+// hist.cu -- exact (value, count) histograms of many value segments.
+//
+// Reference: libdress/src/dress_histogram.c:40-155 -- a hash map keyed on the
+// exact double (equality by ==) flattened to [bits, count] pairs sorted
+// ascending by value.  Here every request's converged edge values sit in one
+// contiguous segment of a device buffer; all segments are sorted at once by a
+// segmented LSD radix sort on the order-preserving 64-bit image of the double
+// (8-bit digits, stable in-tile ranking), then run-length encoded.  Runs are
+// cut where neighbouring values differ under ==, so +0.0/-0.0 merge (they are
+// adjacent after the sort) and every NaN is a run of its own, as in the
+// reference's map.  A pass in which every segment has a single digit value
+// moves nothing and is skipped.
+#include <vector>
+
+#include "engine.h"
+#include "hist.h"
+
+namespace dress {
+namespace {
+
+constexpr int HT = 512;                 // threads per tile block
+constexpr int HI = 16;                  // keys per thread per tile
+constexpr int TILE = HT * HI;           // 8192 keys per tile
+constexpr int RADIX = 256;
+
+__device__ __forceinline__ unsigned long long to_ordered(unsigned long long b)
+{
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
+}
+__device__ __forceinline__ unsigned long long from_ordered(unsigned long long k)
+{
+    return (k >> 63) ? (k & 0x7fffffffffffffffULL) : ~k;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt_h()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+struct Tile {
+    long long begin, end;   // key range
+    int seg;
+};
+
+__global__ void k_to_ordered(long long n, unsigned long long *k)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        k[i] = to_ordered(k[i]);
+}
+
+// per-tile digit counts
+__global__ void __launch_bounds__(HT) k_tile_hist(const Tile *tiles, const unsigned long long *keys,
+                                                  int shift, int *counts)
+{
+    __shared__ int c[RADIX];
+    Tile t = tiles[blockIdx.x];
+    for (int d = threadIdx.x; d < RADIX; d += HT) c[d] = 0;
+    __syncthreads();
+    for (long long i = t.begin + threadIdx.x; i < t.end; i += HT)
+        atomicAdd(&c[(keys[i] >> shift) & 0xff], 1);
+    __syncthreads();
+    for (int d = threadIdx.x; d < RADIX; d += HT) counts[(long long)blockIdx.x * RADIX + d] = c[d];
+}
+
+// per segment: scatter offsets of every (tile, digit); flags a pass that moves keys
+__global__ void __launch_bounds__(RADIX) k_seg_offsets(const long long *seg_begin, const int *seg_tile0,
+                                                       const int *counts, long long *offs, int *moves)
+{
+    __shared__ long long base[RADIX];
+    __shared__ int nonzero;
+    int s = blockIdx.x, d = threadIdx.x;
+    int t0 = seg_tile0[s], t1 = seg_tile0[s + 1];
+    long long tot = 0;
+    for (int t = t0; t < t1; ++t) tot += counts[(long long)t * RADIX + d];
+    if (d == 0) nonzero = 0;
+    base[d] = tot;
+    __syncthreads();
+    if (tot > 0) atomicAdd(&nonzero, 1);
+    if (d == 0) {
+        long long run = seg_begin[s];
+        for (int k = 0; k < RADIX; ++k) {
+            long long c = base[k];
+            base[k] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (nonzero > 1 && d == 0) *moves = 1;
+    long long run = base[d];
+    for (int t = t0; t < t1; ++t) {
+        offs[(long long)t * RADIX + d] = run;
+        run += counts[(long long)t * RADIX + d];
+    }
+}
+
+// stable scatter of one tile: rounds of HT consecutive keys, each key ranked
+// by (its rank among equal digits in its warp) + (same digit in earlier warps
+// of the round) + (same digit in earlier rounds of the tile)
+__global__ void __launch_bounds__(HT) k_tile_scatter(const Tile *tiles, const unsigned long long *src,
+                                                     unsigned long long *dst, int shift,
+                                                     const long long *offs)
+{
+    constexpr int W = HT / 32;
+    __shared__ int wcnt[W][RADIX];
+    __shared__ int rtot[RADIX];
+    __shared__ long long dbase[RADIX];
+    Tile t = tiles[blockIdx.x];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < RADIX; d += HT) dbase[d] = offs[(long long)blockIdx.x * RADIX + d];
+    for (long long r0 = t.begin; r0 < t.end; r0 += HT) {
+        for (int q = threadIdx.x; q < W * RADIX; q += HT) (&wcnt[0][0])[q] = 0;
+        __syncthreads();
+        long long i = r0 + threadIdx.x;
+        bool valid = i < t.end;
+        unsigned long long key = valid ? src[i] : 0ULL;
+        int dg = valid ? (int)((key >> shift) & 0xff) : RADIX;      // RADIX: no key
+        unsigned peers = __match_any_sync(0xffffffffu, dg);
+        int rank = __popc(peers & lanemask_lt_h());
+        if (valid && rank == 0) wcnt[wid][dg] = __popc(peers);
+        __syncthreads();
+        for (int d = threadIdx.x; d < RADIX; d += HT) {
+            int run = 0;
+            for (int w = 0; w < W; ++w) {
+                int c = wcnt[w][d];
+                wcnt[w][d] = run;
+                run += c;
+            }
+            rtot[d] = run;
+        }
+        __syncthreads();
+        if (valid) dst[dbase[dg] + wcnt[wid][dg] + rank] = key;
+        __syncthreads();
+        for (int d = threadIdx.x; d < RADIX; d += HT) dbase[d] += rtot[d];
+        __syncthreads();
+    }
+}
+
+// run heads per tile (segments start a run; == decides equality)
+__device__ __forceinline__ bool is_head(const unsigned long long *k, long long i, long long seg_begin)
+{
+    if (i == seg_begin) return true;
+    double a = __longlong_as_double((long long)from_ordered(k[i]));
+    double b = __longlong_as_double((long long)from_ordered(k[i - 1]));
+    return !(a == b);
+}
+
+__global__ void __launch_bounds__(HT) k_tile_heads(const Tile *tiles, const long long *seg_begin,
+                                                   const unsigned long long *keys, long long *tile_heads)
+{
+    __shared__ int cnt;
+    Tile t = tiles[blockIdx.x];
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    long long sb = seg_begin[t.seg];
+    int c = 0;
+    for (long long i = t.begin + threadIdx.x; i < t.end; i += HT) c += is_head(keys, i, sb);
+    atomicAdd(&cnt, c);
+    __syncthreads();
+    if (threadIdx.x == 0) tile_heads[blockIdx.x] = cnt;
+}
+
+// write (value bits, start) of every run in order; counts follow from starts
+__global__ void __launch_bounds__(HT) k_tile_runs(const Tile *tiles, const long long *seg_begin,
+                                                  const unsigned long long *keys, const long long *tile_base,
+                                                  long long *run_start, unsigned long long *run_bits,
+                                                  int *run_seg)
+{
+    __shared__ int wsum[HT / 32];
+    __shared__ long long carry;
+    Tile t = tiles[blockIdx.x];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    long long sb = seg_begin[t.seg];
+    if (threadIdx.x == 0) carry = tile_base[blockIdx.x];
+    __syncthreads();
+    for (long long r0 = t.begin; r0 < t.end; r0 += HT) {
+        long long i = r0 + threadIdx.x;
+        bool h = i < t.end && is_head(keys, i, sb);
+        unsigned b = __ballot_sync(0xffffffffu, h);
+        if (lane == 0) wsum[wid] = __popc(b);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < HT / 32; ++w) {
+            int c = wsum[w];
+            if (w < wid) before += c;
+            total += c;
+        }
+        if (h) {
+            long long r = carry + before + __popc(b & lanemask_lt_h());
+            run_start[r] = i;
+            run_bits[r] = from_ordered(keys[i]);
+            run_seg[r] = t.seg;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+}
+
+__global__ void k_run_pairs(long long R, const long long *run_start, const unsigned long long *run_bits,
+                            const int *run_seg, const long long *seg_end, long long *pairs)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < R;
+         r += (long long)gridDim.x * blockDim.x) {
+        int s = run_seg[r];
+        long long end = (r + 1 < R && run_seg[r + 1] == s) ? run_start[r + 1] : seg_end[s];
+        pairs[2 * r] = (long long)run_bits[r];
+        pairs[2 * r + 1] = end - run_start[r];
+    }
+}
+
+}  // namespace
+
+Status histogram_segments(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
+                          const std::vector<long long> &len, std::vector<std::vector<long long>> &out,
+                          cudaStream_t st, int sms)
+{
+    const int nseg = (int)begin.size();
+    out.assign((size_t)nseg, std::vector<long long>());
+    std::vector<Tile> tiles;
+    std::vector<int> seg_tile0((size_t)nseg + 1, 0);
+    std::vector<long long> seg_end((size_t)nseg);
+    long long total = 0, lo = -1, hi = 0;
+    for (int s = 0; s < nseg; ++s) {
+        seg_tile0[(size_t)s] = (int)tiles.size();
+        seg_end[(size_t)s] = begin[(size_t)s] + len[(size_t)s];
+        for (long long b = begin[(size_t)s]; b < seg_end[(size_t)s]; b += TILE)
+            tiles.push_back({b, b + TILE < seg_end[(size_t)s] ? b + TILE : seg_end[(size_t)s], s});
+        total += len[(size_t)s];
+        if (len[(size_t)s] > 0) {
+            if (lo < 0 || begin[(size_t)s] < lo) lo = begin[(size_t)s];
+            if (seg_end[(size_t)s] > hi) hi = seg_end[(size_t)s];
+        }
+    }
+    seg_tile0[(size_t)nseg] = (int)tiles.size();
+    if (total == 0) return Status::Ok();
+    const int nt = (int)tiles.size();
+
+    DevBuf<Tile> d_tiles;
+    DevBuf<int> d_seg_tile0, d_counts, d_moves, d_run_seg;
+    DevBuf<long long> d_seg_begin, d_seg_end, d_offs, d_tile_heads, d_tile_base, d_scan_tmp, d_run_start, d_pairs;
+    DevBuf<unsigned long long> d_run_bits;
+    DRESS_TRY(d_tiles.alloc((size_t)nt, st));
+    DRESS_TRY(d_seg_tile0.alloc((size_t)nseg + 1, st));
+    DRESS_TRY(d_seg_begin.alloc((size_t)nseg, st));
+    DRESS_TRY(d_seg_end.alloc((size_t)nseg, st));
+    DRESS_TRY(d_counts.alloc((size_t)nt * RADIX, st));
+    DRESS_TRY(d_offs.alloc((size_t)nt * RADIX, st));
+    DRESS_TRY(d_moves.alloc(1, st));
+    DRESS_CUDA_TRY(cudaMemcpyAsync(d_tiles.get(), tiles.data(), (size_t)nt * sizeof(Tile), cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(cudaMemcpyAsync(d_seg_tile0.get(), seg_tile0.data(), ((size_t)nseg + 1) * sizeof(int),
+                                   cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(cudaMemcpyAsync(d_seg_begin.get(), begin.data(), (size_t)nseg * sizeof(long long),
+                                   cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(cudaMemcpyAsync(d_seg_end.get(), seg_end.data(), (size_t)nseg * sizeof(long long),
+                                   cudaMemcpyHostToDevice, st));
+
+    // order-preserving image of the doubles over the used span
+    k_to_ordered<<<(unsigned)((hi - lo + 255) / 256 < 64 * sms ? (hi - lo + 255) / 256 : 64 * sms), 256, 0, st>>>(
+        hi - lo, keys + lo);
+    unsigned long long *a = keys, *b = alt;
+    for (int pass = 0; pass < 8; ++pass) {
+        int shift = 8 * pass;
+        k_tile_hist<<<nt, HT, 0, st>>>(d_tiles.get(), a, shift, d_counts.get());
+        DRESS_CUDA_TRY(cudaMemsetAsync(d_moves.get(), 0, sizeof(int), st));
+        k_seg_offsets<<<nseg, RADIX, 0, st>>>(d_seg_begin.get(), d_seg_tile0.get(), d_counts.get(), d_offs.get(),
+                                              d_moves.get());
+        int moves = 0;
+        DRESS_CUDA_TRY(cudaMemcpyAsync(&moves, d_moves.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+        if (!moves) continue;
+        k_tile_scatter<<<nt, HT, 0, st>>>(d_tiles.get(), a, b, shift, d_offs.get());
+        unsigned long long *t = a;
+        a = b;
+        b = t;
+    }
+    DRESS_CUDA_TRY(cudaGetLastError());
+
+    // run-length encode
+    DRESS_TRY(d_tile_heads.alloc((size_t)nt, st));
+    DRESS_TRY(d_tile_base.alloc((size_t)nt + 1, st));
+    DRESS_TRY(d_scan_tmp.alloc(scan_tmp_elems(nt), st));
+    k_tile_heads<<<nt, HT, 0, st>>>(d_tiles.get(), d_seg_begin.get(), a, d_tile_heads.get());
+    DRESS_TRY(exclusive_scan_i64(d_tile_heads.get(), d_tile_base.get(), nt, d_scan_tmp.get(), st));
+    long long R = 0;
+    DRESS_CUDA_TRY(cudaMemcpyAsync(&R, d_tile_base.get() + nt, sizeof(R), cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    DRESS_TRY(d_run_start.alloc((size_t)R, st));
+    DRESS_TRY(d_run_bits.alloc((size_t)R, st));
+    DRESS_TRY(d_run_seg.alloc((size_t)R, st));
+    DRESS_TRY(d_pairs.alloc(2 * (size_t)R, st));
+    k_tile_runs<<<nt, HT, 0, st>>>(d_tiles.get(), d_seg_begin.get(), a, d_tile_base.get(), d_run_start.get(),
+                                   d_run_bits.get(), d_run_seg.get());
+    k_run_pairs<<<(unsigned)((R + 255) / 256 < 64 * sms ? (R + 255) / 256 : 64 * sms), 256, 0, st>>>(
+        R, d_run_start.get(), d_run_bits.get(), d_run_seg.get(), d_seg_end.get(), d_pairs.get());
+    DRESS_CUDA_TRY(cudaGetLastError());
+    std::vector<long long> pairs(2 * (size_t)R);
+    std::vector<int> rseg((size_t)R);
+    DRESS_CUDA_TRY(cudaMemcpyAsync(pairs.data(), d_pairs.get(), 2 * (size_t)R * sizeof(long long),
+                                   cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(cudaMemcpyAsync(rseg.data(), d_run_seg.get(), (size_t)R * sizeof(int), cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    for (long long r = 0; r < R; ++r) {
+        auto &v = out[(size_t)rseg[(size_t)r]];
+        v.push_back(pairs[2 * (size_t)r]);
+        v.push_back(pairs[2 * (size_t)r + 1]);
+    }
+    return Status::Ok();
+}
+
+}  // namespace dress

@@ -1,0 +1,277 @@
+"""B200 DRESS engine -- Python mirror of the reference's ``dress.cuda`` API.
+
+Same entry points, argument names, defaults and result fields as
+``python/src/dress/cuda/__init__.py`` of the reference (``fit`` :451,
+``delta_fit`` :497, ``nabla_fit`` :370, ``dress_cuda`` :239,
+``dress_fit_cuda`` :306), all running through ``libdress_cuda.so``'s C ABI.
+``delta_fit_many`` / ``nabla_fit_many`` add what the reference cannot do:
+many graphs' histograms in one persistent launch.
+"""
+import ctypes
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from . import _abi
+
+UNDIRECTED, DIRECTED, FORWARD, BACKWARD = 0, 1, 2, 3
+DELTA, NABLA = 0, 1
+
+_libc = ctypes.CDLL(None)
+_libc.malloc.restype = ctypes.c_void_p
+_libc.malloc.argtypes = [ctypes.c_size_t]
+_libc.free.argtypes = [ctypes.c_void_p]
+
+
+class DressError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dress_b200 error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    return _abi.load()
+
+
+def is_available():
+    """True when the engine library loads and a CUDA device is visible."""
+    try:
+        lib()
+    except (RuntimeError, OSError):
+        return False
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except ImportError:
+        return True
+
+
+def _malloc_copy(arr, ctype):
+    arr = np.ascontiguousarray(arr)
+    raw = _libc.malloc(max(1, arr.nbytes))
+    if not raw:
+        raise MemoryError("malloc failed")
+    if arr.nbytes:
+        ctypes.memmove(raw, arr.ctypes.data, arr.nbytes)
+    return ctypes.cast(raw, ctypes.POINTER(ctype))
+
+
+def _arr(ptr, n, dtype):
+    if n <= 0 or not ptr:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
+
+
+class Graph:
+    """Owns one ``dress_graph_t`` built by the library's ``dress_init_graph``."""
+
+    def __init__(self, n_vertices, sources, targets, weights=None, vertex_weights=None,
+                 variant=UNDIRECTED, precompute_intercepts=False):
+        U = np.asarray(sources, dtype=np.int32)
+        V = np.asarray(targets, dtype=np.int32)
+        if U.shape != V.shape:
+            raise ValueError("sources and targets differ in length")
+        pW = _malloc_copy(np.asarray(weights, dtype=np.float64), ctypes.c_double) if weights is not None else None
+        pNW = (_malloc_copy(np.asarray(vertex_weights, dtype=np.float64), ctypes.c_double)
+               if vertex_weights is not None else None)
+        self.ptr = lib().dress_init_graph(int(n_vertices), int(U.size), _malloc_copy(U, ctypes.c_int),
+                                          _malloc_copy(V, ctypes.c_int), pW, pNW, int(variant),
+                                          int(bool(precompute_intercepts)))
+        if not self.ptr:
+            raise ValueError("dress_init_graph rejected the graph (vertex id out of range?)")
+        self.N = int(n_vertices)
+        self.E = int(U.size)
+
+    @property
+    def edge_dress(self):
+        return _arr(self.ptr.contents.edge_dress, self.E, np.float64)
+
+    @property
+    def vertex_dress(self):
+        return _arr(self.ptr.contents.vertex_dress, self.N, np.float64)
+
+    @property
+    def edge_weight(self):
+        return _arr(self.ptr.contents.edge_weight, self.E, np.float64)
+
+    def close(self):
+        if self.ptr:
+            lib().dress_free_graph(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+@dataclass
+class DRESSResult:
+    sources: list
+    targets: list
+    edge_dress: list
+    edge_weight: list
+    vertex_dress: list
+    iterations: int
+    delta: float
+
+
+@dataclass
+class DeltaDRESSResult:
+    histogram: List[Tuple[float, int]]
+    multisets: Optional[np.ndarray] = None
+    num_subgraphs: int = 0
+    flat: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int64))
+
+
+@dataclass
+class NablaDRESSResult:
+    histogram: List[Tuple[float, int]]
+    multisets: Optional[np.ndarray] = None
+    num_tuples: int = 0
+    flat: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int64))
+
+
+def _check(code):
+    if code != 0:
+        c, msg = _abi.last_error()
+        raise DressError(code, msg)
+
+
+def fit_graph(g: Graph, max_iterations=100, epsilon=1e-6):
+    """GPU fit of an existing graph in place; returns (iterations, delta)."""
+    it, dl = ctypes.c_int(0), ctypes.c_double(0.0)
+    _check(lib().dressx_fit(g.ptr, int(max_iterations), float(epsilon), ctypes.byref(it), ctypes.byref(dl)))
+    return it.value, dl.value
+
+
+def last_fit_stats():
+    st = _abi.FitStats()
+    lib().dressx_last_fit_stats(ctypes.byref(st))
+    return dict(common_terms=st.common_terms, sweeps=st.sweeps, setup_ms=st.setup_ms, iterate_ms=st.iterate_ms)
+
+
+def dress_cuda(N, E, U, V, W=None, NW=None, variant=UNDIRECTED, precompute_intercepts=0,
+               max_iterations=100, epsilon=1e-10):
+    """(edge_dress, vertex_dress, edge_weight, iterations, delta) -- reference
+    ``python/src/dress/cuda/__init__.py:239-303``."""
+    with Graph(N, list(U)[:E] if not isinstance(U, np.ndarray) else U[:E],
+               list(V)[:E] if not isinstance(V, np.ndarray) else V[:E], W, NW, variant,
+               precompute_intercepts) as g:
+        it, dl = fit_graph(g, max_iterations, epsilon)
+        return g.edge_dress, g.vertex_dress, g.edge_weight, it, dl
+
+
+def dress_fit_cuda(g_ptr, max_iterations=100, epsilon=1e-10):
+    """Fit a raw ``dress_graph_t`` pointer (reference :306-326)."""
+    it, dl = ctypes.c_int(0), ctypes.c_double(0.0)
+    lib().dress_fit_cuda(g_ptr, int(max_iterations), float(epsilon), ctypes.byref(it), ctypes.byref(dl))
+    return it.value, dl.value
+
+
+def fit(n_vertices, sources, targets, weights=None, vertex_weights=None, variant=UNDIRECTED,
+        max_iterations=100, epsilon=1e-6, precompute_intercepts=False):
+    """GPU DRESS fit -- reference ``dress.cuda.fit`` (:451-494)."""
+    src, tgt = list(sources), list(targets)
+    with Graph(n_vertices, src, tgt, weights, vertex_weights, variant, precompute_intercepts) as g:
+        it, dl = fit_graph(g, max_iterations, epsilon)
+        return DRESSResult(sources=src, targets=tgt, edge_dress=g.edge_dress.tolist(),
+                           edge_weight=g.edge_weight.tolist(), vertex_dress=g.vertex_dress.tolist(),
+                           iterations=it, delta=dl)
+
+
+def _flat_to_list(flat):
+    if flat.size == 0:
+        return []
+    f = flat.reshape(-1, 2)
+    vals = f[:, 0].copy().view(np.float64)
+    return [(float(v), int(c)) for v, c in zip(vals, f[:, 1])]
+
+
+def hist_requests(graphs, kind, k, max_iterations=100, epsilon=1e-6, n_samples=0, seed=0,
+                  keep_multisets=False, offset=0, stride=1, compute_histogram=True, per_fit=False):
+    """Run one Delta/Nabla request per graph in a single engine call.
+
+    Returns a list of (flat int64 [bits, count, ...], multisets or None,
+    num_subgraphs, fits)."""
+    n = len(graphs)
+    reqs = (_abi.HistRequest * n)()
+    for i, g in enumerate(graphs):
+        r = reqs[i]
+        r.graph = g.ptr
+        r.kind = int(kind)
+        r.k = int(k)
+        r.max_iterations = int(max_iterations)
+        r.epsilon = float(epsilon)
+        r.n_samples = int(n_samples)
+        r.seed = int(seed) & 0xFFFFFFFF
+        r.offset = int(offset)
+        r.stride = int(stride)
+        r.want_histogram = 1 if compute_histogram else 0
+        r.keep_multisets = 1 if keep_multisets else 0
+    fn = lib().dressx_hist_batch_per_fit if per_fit else lib().dressx_hist_batch
+    code = fn(reqs, n)
+    out = []
+    for i, g in enumerate(graphs):
+        r = reqs[i]
+        flat = _arr(r.hist_flat, r.hist_len, np.int64)
+        if r.hist_flat:
+            lib().dressx_free(ctypes.cast(r.hist_flat, ctypes.c_void_p))
+        ms = None
+        if r.multisets:
+            ms = _arr(r.multisets, r.num_subgraphs * g.E, np.float64).reshape(r.num_subgraphs, g.E)
+            lib().dressx_free(ctypes.cast(r.multisets, ctypes.c_void_p))
+        out.append((flat, ms, r.num_subgraphs, r.fits, r.status))
+    _check(code)
+    return out
+
+
+def _graph_args(n_vertices, sources, targets, weights, vertex_weights, variant, precompute):
+    return Graph(n_vertices, sources, targets, weights, vertex_weights, variant, precompute)
+
+
+def delta_fit(n_vertices, sources, targets, weights=None, vertex_weights=None, k=0, variant=UNDIRECTED,
+              max_iterations=100, epsilon=1e-6, precompute=False, keep_multisets=False, offset=0, stride=1,
+              n_samples=0, seed=0, compute_histogram=True):
+    """GPU Delta^k-DRESS -- reference ``dress.cuda.delta_fit`` (:497-575)."""
+    with _graph_args(n_vertices, sources, targets, weights, vertex_weights, variant, precompute) as g:
+        flat, ms, ns, _, _ = hist_requests([g], DELTA, k, max_iterations, epsilon, n_samples, seed,
+                                           keep_multisets, offset, stride, compute_histogram)[0]
+        return DeltaDRESSResult(histogram=_flat_to_list(flat), multisets=ms, num_subgraphs=ns, flat=flat)
+
+
+def nabla_fit(n_vertices, sources, targets, weights=None, vertex_weights=None, k=0, variant=UNDIRECTED,
+              max_iterations=100, epsilon=1e-6, precompute=False, keep_multisets=False, n_samples=0, seed=0,
+              compute_histogram=True, offset=0, stride=1):
+    """GPU Nabla^k-DRESS -- reference ``dress.cuda.nabla_fit`` (:370-445)."""
+    with _graph_args(n_vertices, sources, targets, weights, vertex_weights, variant, precompute) as g:
+        flat, ms, ns, _, _ = hist_requests([g], NABLA, k, max_iterations, epsilon, n_samples, seed,
+                                           keep_multisets, offset, stride, compute_histogram)[0]
+        return NablaDRESSResult(histogram=_flat_to_list(flat), multisets=ms, num_tuples=ns, flat=flat)
+
+
+def delta_fit_many(graphs, k=1, **kw):
+    """Delta^k histograms of many ``Graph`` objects in one persistent launch;
+    returns a list of flat int64 [bits, count, ...] arrays."""
+    return [r[0] for r in hist_requests(graphs, DELTA, k, **kw)]
+
+
+def nabla_fit_many(graphs, k=1, **kw):
+    return [r[0] for r in hist_requests(graphs, NABLA, k, **kw)]
+
+
+def configure(device=-1, memory_budget_bytes=0, fit_chunk=0, group_threads=0):
+    cfg = _abi.Config()
+    cfg.device = int(device)
+    cfg.memory_budget_bytes = int(memory_budget_bytes)
+    cfg.fit_chunk = int(fit_chunk)
+    cfg.group_threads = int(group_threads)
+    _check(lib().dressx_configure(ctypes.byref(cfg)))

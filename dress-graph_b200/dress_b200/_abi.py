@@ -1,0 +1,115 @@
+"""ctypes binding of libdress_cuda.so (the B200 engine's C ABI).
+
+The structures mirror ``include/dress_b200.h`` (which is ABI-identical to the
+reference's ``libdress/include/dress/dress.h:12-75``).  Loading fails loudly
+when the library has not been built: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libdress_cuda.so")
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_dbl_p = ctypes.POINTER(ctypes.c_double)
+_c_i64_p = ctypes.POINTER(ctypes.c_int64)
+
+
+class DressGraph(ctypes.Structure):
+    _fields_ = [
+        ("variant", ctypes.c_int), ("N", ctypes.c_int), ("E", ctypes.c_int),
+        ("U", _c_int_p), ("V", _c_int_p),
+        ("adj_offset", _c_int_p), ("adj_target", _c_int_p), ("adj_edge_idx", _c_int_p),
+        ("max_degree", ctypes.c_int),
+        ("W", _c_dbl_p), ("edge_weight", _c_dbl_p), ("edge_dress", _c_dbl_p),
+        ("edge_dress_next", _c_dbl_p), ("NW", _c_dbl_p), ("vertex_dress", _c_dbl_p),
+        ("precompute_intercepts", ctypes.c_int),
+        ("intercept_offset", _c_int_p), ("intercept_edge_ux", _c_int_p),
+        ("intercept_edge_vx", _c_int_p),
+    ]
+
+
+PGraph = ctypes.POINTER(DressGraph)
+
+
+class HistPair(ctypes.Structure):
+    _fields_ = [("value", ctypes.c_double), ("count", ctypes.c_int64)]
+
+
+class HistRequest(ctypes.Structure):
+    _fields_ = [
+        ("graph", PGraph), ("kind", ctypes.c_int), ("k", ctypes.c_int),
+        ("max_iterations", ctypes.c_int), ("epsilon", ctypes.c_double),
+        ("n_samples", ctypes.c_int), ("seed", ctypes.c_uint),
+        ("offset", ctypes.c_int), ("stride", ctypes.c_int),
+        ("want_histogram", ctypes.c_int), ("keep_multisets", ctypes.c_int),
+        ("hist_flat", _c_i64_p), ("hist_len", ctypes.c_int),
+        ("multisets", _c_dbl_p), ("num_subgraphs", ctypes.c_int64),
+        ("fits", ctypes.c_int64), ("status", ctypes.c_int),
+    ]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int), ("memory_budget_bytes", ctypes.c_size_t),
+        ("fit_chunk", ctypes.c_int), ("group_threads", ctypes.c_int),
+        ("reserved", ctypes.c_int * 8),
+    ]
+
+
+class FitStats(ctypes.Structure):
+    _fields_ = [("common_terms", ctypes.c_int64), ("sweeps", ctypes.c_int),
+                ("setup_ms", ctypes.c_double), ("iterate_ms", ctypes.c_double)]
+
+
+_HIST_ARGS = [PGraph, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+              ctypes.c_uint, _c_int_p, ctypes.c_int, ctypes.POINTER(_c_dbl_p), _c_i64_p]
+
+# name -> (restype, argtypes); every entry point declared in include/*.h
+SIGNATURES = {
+    "dress_init_graph": (PGraph, [ctypes.c_int, ctypes.c_int, _c_int_p, _c_int_p, _c_dbl_p,
+                                  _c_dbl_p, ctypes.c_int, ctypes.c_int]),
+    "dress_free_graph": (None, [PGraph]),
+    "dress_fit": (None, [PGraph, ctypes.c_int, ctypes.c_double, _c_int_p, _c_dbl_p]),
+    "dress_fit_cuda": (None, [PGraph, ctypes.c_int, ctypes.c_double, _c_int_p, _c_dbl_p]),
+    "dress_delta_fit_cuda": (ctypes.POINTER(HistPair), _HIST_ARGS),
+    "dress_delta_fit_cuda_strided": (ctypes.POINTER(HistPair), _HIST_ARGS + [ctypes.c_int, ctypes.c_int]),
+    "dress_delta_fit_cuda_strided_flat": (_c_i64_p, _HIST_ARGS + [ctypes.c_int, ctypes.c_int]),
+    "dress_delta_fit_cuda_flat": (_c_i64_p, _HIST_ARGS),
+    "dress_nabla_fit_cuda": (ctypes.POINTER(HistPair), _HIST_ARGS),
+    "dress_nabla_fit_cuda_strided": (ctypes.POINTER(HistPair), _HIST_ARGS + [ctypes.c_int, ctypes.c_int]),
+    "dress_nabla_fit_cuda_flat": (_c_i64_p, _HIST_ARGS),
+    "dress_nabla_fit_cuda_strided_flat": (_c_i64_p, _HIST_ARGS + [ctypes.c_int, ctypes.c_int]),
+    "dressx_configure": (ctypes.c_int, [ctypes.POINTER(Config)]),
+    "dressx_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int]),
+    "dressx_fit": (ctypes.c_int, [PGraph, ctypes.c_int, ctypes.c_double, _c_int_p, _c_dbl_p]),
+    "dressx_last_fit_stats": (ctypes.c_int, [ctypes.POINTER(FitStats)]),
+    "dressx_hist_batch": (ctypes.c_int, [ctypes.POINTER(HistRequest), ctypes.c_int]),
+    "dressx_hist_batch_per_fit": (ctypes.c_int, [ctypes.POINTER(HistRequest), ctypes.c_int]),
+    "dressx_free": (None, [ctypes.c_void_p]),
+}
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    """Load and bind the engine library (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libdress_cuda.so not built at {path}; run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error():
+    lib = load()
+    buf = ctypes.create_string_buffer(512)
+    code = lib.dressx_last_error(buf, 512)
+    return code, buf.value.decode(errors="replace")

@@ -1,0 +1,144 @@
+"""GPU parity of the Delta^k / Nabla^k histograms against the oracle.
+
+Bar: identical exact (value bits, count) lists, identical num_subgraphs and
+bit-identical multiset rows.
+"""
+import ctypes
+import gzip
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import dress_b200 as db
+from dress_b200 import graphs
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def bits(a):
+    return np.asarray(a, dtype=np.float64).view(np.int64)
+
+
+def gpu_hist(kind, n, U, V, W=None, variant=0, per_fit=False, **kw):
+    with db.Graph(n, U, V, W, None, variant) as g:
+        flat, ms, num, fits, status = db.hist_requests([g], kind, per_fit=per_fit, **kw)[0]
+        return dict(hist=flat, multisets=ms, num=num, fits=fits)
+
+
+def test_golden_histograms():
+    with gzip.open(os.path.join(ROOT, "tests", "golden", "hist_cases.json.gz"), "rt") as f:
+        cases = json.load(f)
+    for c in cases:
+        kind = db.DELTA if c["kind"] == "delta" else db.NABLA
+        r = gpu_hist(kind, c["N"], c["U"], c["V"], c["W"], c["variant"], k=c["k"], n_samples=c["n_samples"],
+                     seed=c["seed"], offset=c["offset"], stride=c["stride"], keep_multisets=True)
+        assert r["num"] == c["num"], c
+        np.testing.assert_array_equal(r["hist"], np.asarray(c["hist"], np.int64), err_msg=str(c["name"]))
+        if c["multisets"] is not None:
+            np.testing.assert_array_equal(bits(r["multisets"].ravel()), c["multisets"])
+
+
+def test_batch_of_regular_graphs_delta1(oracle_port):
+    """The batched-Delta^1 workload in small: random d-regular graphs of
+    uneven size in one call, each histogram exact."""
+    gs = graphs.regular_batch(40, (16, 60), (3, 12), seed=5)
+    objs = [db.Graph(n, U, V) for n, U, V in gs]
+    flats = db.delta_fit_many(objs, k=1)
+    for (n, U, V), flat in zip(gs, flats):
+        ref = oracle_port.delta_fit(n, U, V, k=1)
+        np.testing.assert_array_equal(flat, ref["hist"])
+    for g in objs:
+        g.close()
+
+
+@pytest.mark.parametrize("kind", [db.DELTA, db.NABLA])
+@pytest.mark.parametrize("k", [1, 2])
+def test_regular_graph_k12(oracle_port, kind, k):
+    n, U, V = graphs.random_regular(40, 10, seed=3)
+    W = graphs.uniform_weights(len(U), seed=3)
+    fn = oracle_port.delta_fit if kind == db.DELTA else oracle_port.nabla_fit
+    for w in (None, W):
+        r = gpu_hist(kind, n, U, V, w, k=k)
+        ref = fn(n, U, V, w, k=k)
+        np.testing.assert_array_equal(r["hist"], ref["hist"])
+        assert r["num"] == ref["num"]
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_variants_strides_sampling_multisets(oracle_port, variant):
+    n, U, V = graphs.erdos_renyi(24, 70, seed=variant + 1)
+    W = graphs.uniform_weights(len(U), seed=9)
+    for kind, fn in ((db.DELTA, oracle_port.delta_fit), (db.NABLA, oracle_port.nabla_fit)):
+        for k, ns, seed, off, st in ((1, 0, 0, 0, 1), (2, 0, 0, 1, 3), (2, 17, 5, 0, 1), (2, 11, 2, 2, 4)):
+            r = gpu_hist(kind, n, U, V, W, variant, k=k, n_samples=ns, seed=seed, offset=off, stride=st,
+                         keep_multisets=True)
+            ref = fn(n, U, V, W, k=k, n_samples=ns, seed=seed, offset=off, stride=st, keep_multisets=True,
+                     variant=variant)
+            np.testing.assert_array_equal(r["hist"], ref["hist"])
+            assert r["num"] == ref["num"]
+            np.testing.assert_array_equal(bits(r["multisets"]), bits(ref["multisets"]))
+
+
+def test_per_fit_path_matches_batched(oracle_port):
+    n, U, V = graphs.random_regular(30, 6, seed=2)
+    a = gpu_hist(db.DELTA, n, U, V, k=1)
+    b = gpu_hist(db.DELTA, n, U, V, k=1, per_fit=True)
+    np.testing.assert_array_equal(a["hist"], b["hist"])
+    assert a["fits"] == b["fits"] == n
+
+
+def test_wide_rows_use_per_fit_path(oracle_port):
+    """A parent with a 40-neighbour vertex is outside the batched kernel's
+    register networks and runs through the per-subgraph path."""
+    n = 41
+    U = np.array([0] * 40 + list(range(1, 40)), np.int32)
+    V = np.array(list(range(1, 41)) + list(range(2, 41)), np.int32)
+    ref = oracle_port.delta_fit(n, U, V, k=1)
+    r = gpu_hist(db.DELTA, n, U, V, k=1)
+    np.testing.assert_array_equal(r["hist"], ref["hist"])
+
+
+def test_k0_fits_in_place_and_k_ge_n(oracle_port):
+    n, U, V = graphs.erdos_renyi(30, 80, seed=3)
+    with db.Graph(n, U, V) as g:
+        flat, ms, num, _, _ = db.hist_requests([g], db.DELTA, 0, keep_multisets=True)[0]
+        ref = oracle_port.delta_fit(n, U, V, k=0, keep_multisets=True)
+        np.testing.assert_array_equal(flat, ref["hist"])
+        assert num == 1
+        # the caller's graph holds the fitted values afterwards
+        np.testing.assert_array_equal(bits(g.edge_dress), bits(ref["multisets"][0]))
+    for kind in (db.DELTA, db.NABLA):
+        r = gpu_hist(kind, n, U, V, k=n)
+        assert r["hist"].size == 0
+
+
+def test_legacy_pair_entry_points(oracle_port):
+    n, U, V = graphs.random_regular(16, 4, seed=1)
+    lib = db.lib()
+    with db.Graph(n, U, V) as g:
+        hs = ctypes.c_int(0)
+        ns = ctypes.c_int64(0)
+        ms = ctypes.POINTER(ctypes.c_double)()
+        p = lib.dress_delta_fit_cuda(g.ptr, 1, 100, 1e-6, 0, 0, ctypes.byref(hs), 0, ctypes.byref(ms),
+                                     ctypes.byref(ns))
+        ref = oracle_port.delta_fit(n, U, V, k=1)
+        pairs = [(p[i].value, p[i].count) for i in range(hs.value)]
+        lib.dressx_free(ctypes.cast(p, ctypes.c_void_p))
+        f = np.asarray(ref["hist"]).reshape(-1, 2)
+        assert [(float(v), int(c)) for v, c in zip(f[:, 0].copy().view(np.float64), f[:, 1])] == pairs
+        assert ns.value == n
+        # hist_size == NULL: no histogram, NULL result
+        p = lib.dress_nabla_fit_cuda(g.ptr, 1, 100, 1e-6, 0, 0, None, 0, None, ctypes.byref(ns))
+        assert not p
+
+
+def test_reference_delta_test_binary():
+    exe = os.path.join(ROOT, "oracle", "_ref", "test_delta_dress_redirect")
+    if not os.path.exists(exe):
+        pytest.skip("reference test binary not built")
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr

@@ -1,0 +1,155 @@
+"""GPU parity of dress_fit_cuda against the oracle and the golden fixtures.
+
+Bar: bit-identical edge and vertex values, identical iteration count and
+final delta (the reference's own CUDA test accepts 1e-12,
+tests/c/cuda/test_dress_cuda.c:180; this engine is exact).
+"""
+import ctypes
+import gzip
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import dress_b200 as db
+from dress_b200 import graphs
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def bits(a):
+    return np.asarray(a, dtype=np.float64).view(np.int64)
+
+
+def gpu_fit(n, U, V, W=None, NW=None, variant=0, pre=0, max_iterations=100, epsilon=1e-6):
+    with db.Graph(n, U, V, W, NW, variant, pre) as g:
+        it, dl = db.fit_graph(g, max_iterations, epsilon)
+        return dict(edge_dress=g.edge_dress, vertex_dress=g.vertex_dress, iterations=it, delta=dl)
+
+
+def assert_same(a, b, name=""):
+    assert a["iterations"] == b["iterations"], (name, a["iterations"], b["iterations"])
+    assert bits([a["delta"]])[0] == bits([b["delta"]])[0], (name, a["delta"], b["delta"])
+    np.testing.assert_array_equal(bits(a["edge_dress"]), bits(b["edge_dress"]), err_msg=name)
+    np.testing.assert_array_equal(bits(a["vertex_dress"]), bits(b["vertex_dress"]), err_msg=name)
+
+
+def test_golden_fits():
+    with gzip.open(os.path.join(ROOT, "tests", "golden", "fit_cases.json.gz"), "rt") as f:
+        cases = json.load(f)
+    for c in cases:
+        r = gpu_fit(c["N"], c["U"], c["V"], c["W"], None, c["variant"], c["precompute"],
+                    c["max_iterations"], c["eps"])
+        assert r["iterations"] == c["iterations"], c["name"]
+        assert bits([r["delta"]])[0] == c["delta"], c["name"]
+        np.testing.assert_array_equal(bits(r["edge_dress"]), c["edge_dress"], err_msg=c["name"])
+        np.testing.assert_array_equal(bits(r["vertex_dress"]), c["vertex_dress"], err_msg=c["name"])
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("weighted", [False, True])
+def test_er2000_all_variants(oracle_port, variant, weighted):
+    """The plain-fit workload: G(2000, 10000)."""
+    n, U, V = graphs.erdos_renyi(2000, 10000, seed=42)
+    W = graphs.uniform_weights(10000, seed=1) if weighted else None
+    a = gpu_fit(n, U, V, W, variant=variant)
+    b = oracle_port.fit(n, U, V, W, variant=variant)
+    assert_same(a, b)
+
+
+@pytest.mark.parametrize("pre", [0, 1])
+def test_powerlaw_bins(oracle_port, pre):
+    """Chung-Lu graph whose rows and triangle counts fill every bin
+    (thread, warp and block items)."""
+    n, U, V = graphs.chung_lu(20000, 120000, 2.3, 3000, seed=3)
+    W = graphs.uniform_weights(len(U), seed=2)
+    NW = np.random.default_rng(1).uniform(0.5, 2.0, n)
+    a = gpu_fit(n, U, V, W, NW, pre=pre)
+    b = oracle_port.fit(n, U, V, W, NW, precompute=1)
+    assert_same(a, b)
+
+
+def test_hub_row_larger_than_shared_memory(oracle_port):
+    """A star with 40000 leaves: the hub's 40001-term norm spills to global."""
+    n = 40001
+    U = np.zeros(40000, np.int32)
+    V = np.arange(1, 40001, dtype=np.int32)
+    a = gpu_fit(n, U, V)
+    b = oracle_port.fit(n, U, V)
+    assert_same(a, b)
+
+
+def test_multigraph_and_self_loops(oracle_port):
+    rng = np.random.default_rng(9)
+    n = 30
+    U = rng.integers(0, n, 200).astype(np.int32)
+    V = rng.integers(0, n, 200).astype(np.int32)
+    W = rng.uniform(0.5, 2.0, 200)
+    for variant in range(4):
+        assert_same(gpu_fit(n, U, V, W, variant=variant), oracle_port.fit(n, U, V, W, variant=variant), str(variant))
+
+
+def test_degenerate_inputs(oracle_port):
+    # no edges, no vertices, zero iterations, epsilon 0 (all sweeps run)
+    assert_same(gpu_fit(5, [], []), oracle_port.fit(5, [], []))
+    assert_same(gpu_fit(0, [], []), oracle_port.fit(0, [], []))
+    n, U, V = graphs.erdos_renyi(50, 120, seed=4)
+    assert_same(gpu_fit(n, U, V, epsilon=0.0, max_iterations=7),
+                oracle_port.fit(n, U, V, epsilon=0.0, max_iterations=7))
+    with db.Graph(n, U, V) as g:
+        it, _ = db.fit_graph(g, 0, 1e-6)
+        assert it == 0
+        np.testing.assert_array_equal(g.edge_dress, 1.0)
+
+
+def test_fit_continues_from_current_values(oracle_port):
+    """A second call starts from edge_dress, like the reference's dress_fit."""
+    n, U, V = graphs.erdos_renyi(300, 1200, seed=8)
+    with db.Graph(n, U, V) as g:
+        db.fit_graph(g, 3, 1e-6)
+        it, dl = db.fit_graph(g, 100, 1e-9)
+        ed = g.edge_dress
+    gb = oracle_port.build(n, U, V)
+    it0, d0 = ctypes.c_int(), ctypes.c_double()
+    oracle_port.fit_fn(gb, 3, 1e-6, ctypes.byref(it0), ctypes.byref(d0))
+    oracle_port.fit_fn(gb, 100, 1e-9, ctypes.byref(it0), ctypes.byref(d0))
+    ref = np.ctypeslib.as_array(gb.contents.edge_dress, (len(U),)).copy()
+    oracle_port.free_graph(gb)
+    assert it == it0.value and dl == d0.value
+    np.testing.assert_array_equal(bits(ed), bits(ref))
+
+
+def test_python_api_mirror(oracle_port):
+    n, U, V = graphs.erdos_renyi(100, 400, seed=6)
+    r = db.fit(n, U.tolist(), V.tolist(), epsilon=1e-8)
+    b = oracle_port.fit(n, U, V, epsilon=1e-8)
+    assert r.iterations == b["iterations"]
+    np.testing.assert_array_equal(bits(r.edge_dress), bits(b["edge_dress"]))
+    ed, vd, ew, it, dl = db.dress_cuda(n, len(U), U, V, epsilon=1e-8)
+    np.testing.assert_array_equal(bits(ed), bits(b["edge_dress"]))
+
+
+def test_malformed_graph_is_rejected_without_crash():
+    n, U, V = graphs.erdos_renyi(20, 40, seed=1)
+    with db.Graph(n, U, V) as g:
+        g.ptr.contents.adj_edge_idx[3] = 10_000          # out of range edge id
+        with pytest.raises(db.DressError) as e:
+            db.fit_graph(g, 10, 1e-6)
+        assert e.value.code == 1
+    # the engine is still usable afterwards
+    with db.Graph(n, U, V) as g:
+        db.fit_graph(g, 10, 1e-6)
+
+
+def test_reference_cuda_test_binary():
+    """The reference's own tests/c/cuda/test_dress_cuda.c (built from its
+    sources into oracle/_ref) against this library."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "test_dress_cuda")
+    if not os.path.exists(exe):
+        pytest.skip("reference test binary not built")
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "ALL TESTS PASSED" in out.stdout
