@@ -1,0 +1,419 @@
+"""Benchmark of the B200 DRESS engine (one JSON line on rank 0).
+
+Headline workload (BASELINE config "batched Delta^1"): 2,000 random
+d-regular graphs (configuration model with switching repair), n ~ U[16,100],
+d ~ U{3..12}, unweighted, k = 1, epsilon 1e-6, max 100 sweeps, exact
+(value, count) histogram per graph.  One step = all ~115K vertex-deleted
+subgraph fits plus the 2,000 histograms.  Metric: subgraph-fits/s.
+
+* ``value``: the prepared batch (graphs resident in HBM), device time of
+  the fits + histograms from CUDA events on the engine stream, L2 flushed
+  (256 MiB write) between timed steps, outside the timed regions.
+* ``e2e``: the public C-ABI call ``dressx_hist_batch`` with host graphs,
+  wall clock per step: host packing, H2D, fits, histograms, D2H, results.
+* ``per_fit_gpu``: the reference's driver structure with this engine's GPU
+  fit (``dressx_hist_batch_per_fit``: host subgraph build + one fit launch
+  sequence per subgraph) on a bounded sample -- the batched/per-fit ratio.
+* ``cpu_baseline``: the reference's single-thread C ``dress_delta_fit``
+  (compiled from its sources into oracle/_ref) on a bounded sample.
+* ``single_fit``: the 28M-edge Chung-Lu fit (BASELINE config "single large
+  fit"), edge-iters/s and the HBM roofline of its sweeps.
+
+``--impl reference`` times the reference's own CPU implementation
+(``dress_delta_fit_omp``, all host threads) on a bounded sample of the same
+workload.  With ``--gpus N`` (torchrun), the 2,000 graphs are sharded over
+ranks (no collective on the data path); value = all ranks' fits / max time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dress-graph_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--graphs", type=int, default=2000)
+    ap.add_argument("--no-single-fit", action="store_true", help="skip the 28M-edge single fit")
+    ap.add_argument("--single-fit-edges", type=int, default=28_000_000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class Clocks:
+    """Samples nvidia-smi clocks/throttle reasons during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(n_gpus):
+    """Rank/world from torchrun's environment (gloo-free: N=1 needs nothing)."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def allmax(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ---------------------------------------------------------------------------
+# headline: batched Delta^1 over 2,000 random regular graphs
+# ---------------------------------------------------------------------------
+
+def regular_workload(count):
+    from dress_b200 import graphs
+    return graphs.regular_batch(count, (16, 100), (3, 12), seed=42)
+
+
+def cpu_delta1_sample(gs, budget_s, kind):
+    """Reference single-thread Delta^1 on graphs taken in order until the
+    time budget is spent; returns (fits/s, graphs, fits, seconds)."""
+    import oracle
+    cpu = oracle.reference() if kind == "reference" else oracle.port()
+    fits, t0, used = 0, time.perf_counter(), 0
+    for n, U, V in gs:
+        cpu.delta_fit(n, U, V, k=1, max_iterations=100, epsilon=1e-6)
+        fits += n
+        used += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return fits / dt, used, fits, dt
+
+
+def bench_delta1(args, rank, world, pg, torch, clocks):
+    import dress_b200 as db
+    gs_all = regular_workload(args.graphs)
+    mine = gs_all[rank::world]
+    objs = [db.Graph(n, U, V) for n, U, V in mine]
+    stream = torch.cuda.ExternalStream(db.stream_handle())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > L2
+
+    # ---- device throughput, inputs resident --------------------------------
+    db.counters(reset=True)
+    batch = db.Batch(objs, db.DELTA, 1, max_iterations=100, epsilon=1e-6)
+    create = db.counters(reset=True)
+    for _ in range(args.warmup):
+        batch.run()
+    ref_hist = batch.fetch()
+    barrier(pg)
+    torch.cuda.synchronize()
+    clocks.start()
+    dev_ms = fit_ms = hist_ms = 0.0
+    db.counters(reset=True)
+    wall0 = time.perf_counter()
+    for step in range(args.steps):
+        flush.fill_(float(step))
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        batch.run()
+        ev1.record(stream)
+        ev1.synchronize()
+        dev_ms += ev0.elapsed_time(ev1)
+        f, h = batch.timing()
+        fit_ms += f
+        hist_ms += h
+    wall = time.perf_counter() - wall0
+    launches = db.counters()["launches"]
+    torch.cuda.synchronize()
+    barrier(pg)
+    st = batch.stats()
+    fits_step = st["fits"]
+    max_dev_ms = allmax(pg, dev_ms)
+    total_fits = allsum(pg, fits_step * args.steps)
+    value = total_fits / (max_dev_ms / 1e3)
+
+    # ---- end to end through the C ABI, host graphs ---------------------------
+    db.counters(reset=True)
+    e2e_s = 0.0
+    for step in range(args.steps + 1):
+        t0 = time.perf_counter()
+        out = db.hist_requests(objs, db.DELTA, 1, max_iterations=100, epsilon=1e-6)
+        dt = time.perf_counter() - t0
+        if step == 0:                                    # untimed warm-up call
+            db.counters(reset=True)
+            continue
+        e2e_s += dt
+    cnt = db.counters()
+    clk = clocks.stop()            # samples cover the device-timed steps and the e2e calls
+    same = all(np.array_equal(a[0], b) for a, b in zip(out, ref_hist))
+    e2e_s = allmax(pg, e2e_s)
+    e2e_value = total_fits / e2e_s
+    h2d_step = cnt["h2d_bytes"] / args.steps
+    d2h_step = cnt["d2h_bytes"] / args.steps
+
+    # ---- the reference's per-fit structure with this engine's GPU fit ------------
+    per_fit = None
+    if rank == 0:
+        fits, t0, used = 0, time.perf_counter(), 0
+        for g in objs:
+            db.hist_requests([g], db.DELTA, 1, per_fit=True)
+            fits += g.N
+            used += 1
+            if time.perf_counter() - t0 > 8.0:
+                break
+        dt = time.perf_counter() - t0
+        per_fit = {"value": fits / dt, "unit": "subgraph-fits/s", "sample": f"first {used} graphs, {fits} fits",
+                   "batched_over_per_fit": value / (fits / dt)}
+
+    # ---- roofline of the dominant kernel (the batched fit) -----------------------
+    peak, peak_kind = peaks()
+    live_values = sum(n * (len(U) - (2 * len(U)) // n) for n, U, V in mine)   # E - d per subgraph
+    alg_bytes = create["h2d_bytes"] + 8 * live_values                           # parents read + values written
+    achieved = alg_bytes / (fit_ms / args.steps / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "kernel": "k_batch (batched subgraph fits)",
+                "note": "on-chip bound: each subgraph lives in shared memory; HBM carries only the "
+                        "parents and the converged values"}
+
+    for g in objs:
+        g.close()
+    batch.close()
+    return dict(value=value, ms_per_step=max_dev_ms / args.steps, fits_per_step=allsum(pg, fits_step),
+                edge_updates_per_step=allsum(pg, st["edge_updates"]), fit_ms=fit_ms / args.steps,
+                hist_ms=hist_ms / args.steps, wall_ms=wall * 1e3 / args.steps, launches=launches,
+                e2e={"value": e2e_value, "unit": "subgraph-fits/s", "h2d_bytes_per_step": int(h2d_step),
+                     "d2h_bytes_per_step": int(d2h_step), "matches_device_run": bool(same)},
+                per_fit=per_fit, roofline=roofline, clocks=clk, gs=gs_all)
+
+
+# ---------------------------------------------------------------------------
+# single large fit: Chung-Lu 4M vertices / 28M edges
+# ---------------------------------------------------------------------------
+
+def bench_single_fit(args, torch):
+    import dress_b200 as db
+    from dress_b200 import graphs
+    n = 4_000_000 * args.single_fit_edges // 28_000_000
+    n, U, V = graphs.chung_lu(n, args.single_fit_edges, 2.3, 20000, seed=42)
+    E = len(U)
+    out = {"workload": f"Chung-Lu power law, N={n}, E={E}, gamma 2.3, max degree 20000, epsilon 1e-6"}
+    peak, peak_kind = peaks()
+    for label, W in (("weighted", graphs.uniform_weights(E, seed=7)), ("unweighted", None)):
+        g = db.Graph(n, U, V, W)
+        S = int(g.ptr.contents.adj_offset[n])
+        db.counters(reset=True)
+        t0 = time.perf_counter()
+        it, dl = db.fit_graph(g, 100, 1e-6)
+        wall = time.perf_counter() - t0
+        cnt = db.counters()
+        st = db.last_fit_stats()
+        sweeps = st["sweeps"]
+        sweep_ms = st["iterate_ms"] / max(1, sweeps)
+        # algorithmic bytes per sweep: 24N + 12S + 48E weighted, 24N + 12S + 32E unweighted
+        b_iter = 24 * n + 12 * S + (48 if W is not None else 32) * E
+        achieved = b_iter / (sweep_ms / 1e3) / 1e9
+        out[label] = {
+            "iterations": it, "sweeps": sweeps, "delta": dl, "common_terms": st["common_terms"],
+            "edge_iters_per_s": E * sweeps / (st["iterate_ms"] / 1e3),
+            "edge_iters_per_s_e2e": E * sweeps / wall,
+            "sweep_ms": sweep_ms, "setup_ms": st["setup_ms"], "e2e_ms": wall * 1e3,
+            "h2d_bytes": cnt["h2d_bytes"], "d2h_bytes": cnt["d2h_bytes"], "launches": cnt["launches"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_sweep": b_iter},
+        }
+        g.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# the reference arm: the reference's own CPU implementation
+# ---------------------------------------------------------------------------
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    import oracle
+    cpu = oracle.reference()
+    kind = "reference"
+    if cpu is None:
+        cpu, kind = oracle.port(), "port"
+    cores = len(os.sched_getaffinity(0))
+    gs = regular_workload(args.graphs)
+    # a bounded sample per step: consecutive graphs of the workload
+    per_step = max(1, int(os.environ.get("DRESS_REF_GRAPHS", "150")))
+    omp = kind == "reference"
+
+    def step(i):
+        fits = 0
+        base = (i * per_step) % len(gs)
+        for j in range(per_step):
+            n, U, V = gs[(base + j) % len(gs)]
+            cpu.delta_fit(n, U, V, k=1, max_iterations=100, epsilon=1e-6, omp=omp)
+            fits += n
+        return fits
+
+    for i in range(args.warmup):
+        step(i)
+    t0 = time.perf_counter()
+    fits = sum(step(args.warmup + i) for i in range(args.steps))
+    dt = time.perf_counter() - t0
+    v = fits / dt
+    line = {"metric": "Delta^1 subgraph-fits/s", "value": v, "unit": "subgraph-fits/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"batched Delta^1, {per_step} of the {len(gs)} random regular graphs per step "
+                                   "(n~U[16,100], d~U{3..12}), epsilon 1e-6"},
+            "cpu_baseline": {"value": v, "unit": "subgraph-fits/s", "cores": cores if omp else 1, "kind": kind,
+                             "sample": f"{per_step} graphs per step ({'dress_delta_fit_omp' if omp else 'oracle port'})"},
+            "e2e": {"value": v, "unit": "subgraph-fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    rank, world, local, pg = dist_init(args.gpus)
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    import torch
+    torch.cuda.set_device(local)
+    import dress_b200 as db
+    db.configure(device=local)
+    clocks = Clocks(local)
+    head = bench_delta1(args, rank, world, pg, torch, clocks)
+    single = None
+    cpu = None
+    if rank == 0 and world == 1:
+        v, used, fits, dt = cpu_delta1_sample(head["gs"], args.cpu_seconds,
+                                              "reference" if __import__("oracle").reference() else "port")
+        kind = "reference" if __import__("oracle").reference() else "port"
+        cpu = {"value": v, "unit": "subgraph-fits/s", "cores": 1, "kind": kind,
+               "sample": f"single-thread dress_delta_fit on the first {used} graphs ({fits} fits, {dt:.1f} s)"}
+        if not args.no_single_fit:
+            single = bench_single_fit(args, torch)
+    if rank == 0:
+        clk = head["clocks"]
+        line = {
+            "metric": "Delta^1 subgraph-fits/s", "value": head["value"], "unit": "subgraph-fits/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"batched Delta^1 of {args.graphs} random d-regular graphs "
+                                   "(configuration model + switching repair, n~U[16,100], d~U{3..12}, seed 42), "
+                                   "k=1, epsilon 1e-6, max 100 sweeps, exact histogram per graph",
+                       "fits_per_step": head["fits_per_step"], "edge_updates_per_step": head["edge_updates_per_step"],
+                       "l2": "256 MiB flush between timed steps (outside the timed regions)",
+                       "parallelism": f"graphs sharded over {world} GPU(s)"},
+            "e2e": head["e2e"], "gpu_launches": head["launches"], "roofline": head["roofline"],
+            "cpu_baseline": cpu, "per_fit_gpu": head["per_fit"],
+            "breakdown_ms": {"fits": head["fit_ms"], "histograms": head["hist_ms"], "wall": head["wall_ms"]},
+            "clocks": clk, "single_fit": single,
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        barrier(pg)
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -367,7 +367,7 @@ Status launch_m(const BatchLaunch &L, int sms, cudaStream_t st)
     if (per_sm < 1) return Status::Err(DRESSX_EUNSUPPORTED, "batch kernel does not fit on an SM");
     int grid = per_sm * sms;
     if (grid > L.nchunks) grid = L.nchunks;
-    k_batch<M><<<grid, L.gsize * L.groups, smem, st>>>(L);
+    count_launch(), k_batch<M><<<grid, L.gsize * L.groups, smem, st>>>(L);
     DRESS_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
 }

@@ -299,7 +299,7 @@ Status hist_of_host_values(std::vector<Prep *> &ps, cudaStream_t st, int sms)
         begin.push_back(o);
         len.push_back((long long)p->values_host.size());
         if (!p->values_host.empty())
-            DRESS_CUDA_TRY(cudaMemcpyAsync(keys.get() + o, p->values_host.data(),
+            DRESS_CUDA_TRY(counted_memcpy(keys.get() + o, p->values_host.data(),
                                            p->values_host.size() * sizeof(long long), cudaMemcpyHostToDevice, st));
         o += (long long)p->values_host.size();
     }
@@ -327,8 +327,30 @@ Tune pick_tune(int maxE, int maxN, int M, const dressx_config_t &cfg)
     return {gs, groups};
 }
 
-Status run_batched(std::vector<Prep *> &ps, Engine &en)
+// A packed, uploaded batch: parents, chunks, value and statistics buffers.
+struct BatchPlan {
+    std::vector<Prep *> ps;
+    BatchLaunch L{};
+    std::vector<ParentDesc> descs;
+    std::vector<Chunk> chunks;
+    std::vector<long long> val_base;
+    long long values = 0, ms_total = 0;
+    DevBuf<unsigned char> d_pdata;
+    DevBuf<ParentDesc> d_desc;
+    DevBuf<Chunk> d_chunks;
+    DevBuf<long long> d_ranks;
+    DevBuf<unsigned long long> d_vals, d_alt, d_stats;
+    DevBuf<double> d_ms;
+    DevBuf<int> d_counter;
+    std::vector<unsigned long long> stats;
+    HistResult hist;
+    bool need_hist = false;
+    float fit_ms = 0.f, hist_ms = 0.f;       // device time of the last run
+};
+
+Status plan_batched(std::vector<Prep *> &ps, Engine &en, BatchPlan &P)
 {
+    P.ps = ps;
     cudaStream_t st = en.stream;
     int smem_optin = 0;
     DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, en.device));
@@ -337,8 +359,8 @@ Status run_batched(std::vector<Prep *> &ps, Engine &en)
     // one launch for all batchable requests
     int maxE = 1, maxN = 1, maxk = 1, M = 2;
     long long maxbytes = 16, arena = 0, values = 0, ms_total = 0, nranks = 0;
-    std::vector<ParentDesc> descs;
-    std::vector<long long> val_base;
+    std::vector<ParentDesc> &descs = P.descs;
+    std::vector<long long> &val_base = P.val_base;
     for (Prep *p : ps) {
         ParentLayout PL = parent_layout(p->N, p->E, p->S, p->T, 0, 0);
         maxE = std::max(maxE, p->E);
@@ -369,7 +391,7 @@ Status run_batched(std::vector<Prep *> &ps, Engine &en)
         if (p->ms_host) ms_total += p->total * (long long)p->E;
     }
     Tune tu = pick_tune(maxE, maxN, M, en.cfg);
-    BatchLaunch L{};
+    BatchLaunch &L = P.L;
     L.gsize = tu.gsize;
     L.maxE = maxE;
     L.maxN = maxN;
@@ -415,20 +437,22 @@ Status run_batched(std::vector<Prep *> &ps, Engine &en)
         hranks.insert(hranks.end(), p->ranks.begin(), p->ranks.end());
     }
     // chunks: a few rounds of subgraphs per CTA visit
-    std::vector<Chunk> chunks;
+    std::vector<Chunk> &chunks = P.chunks;
     const int chunk_items = 4 * L.groups;
     for (size_t i = 0; i < ps.size(); ++i)
         for (long long f = 0; f < ps[i]->items; f += chunk_items)
             chunks.push_back({(int)i, (int)std::min<long long>(chunk_items, ps[i]->items - f), f});
 
     const int nreq = (int)ps.size();
-    DevBuf<unsigned char> d_pdata;
-    DevBuf<ParentDesc> d_desc;
-    DevBuf<Chunk> d_chunks;
-    DevBuf<long long> d_ranks;
-    DevBuf<unsigned long long> d_vals, d_alt, d_stats;
-    DevBuf<double> d_ms;
-    DevBuf<int> d_counter;
+    DevBuf<unsigned char> &d_pdata = P.d_pdata;
+    DevBuf<ParentDesc> &d_desc = P.d_desc;
+    DevBuf<Chunk> &d_chunks = P.d_chunks;
+    DevBuf<long long> &d_ranks = P.d_ranks;
+    DevBuf<unsigned long long> &d_vals = P.d_vals, &d_stats = P.d_stats;
+    DevBuf<double> &d_ms = P.d_ms;
+    DevBuf<int> &d_counter = P.d_counter;
+    P.values = values;
+    P.ms_total = ms_total;
     DRESS_TRY(d_pdata.alloc((size_t)arena, st));
     DRESS_TRY(d_desc.alloc(descs.size(), st));
     DRESS_TRY(d_chunks.alloc(chunks.size(), st));
@@ -437,23 +461,21 @@ Status run_batched(std::vector<Prep *> &ps, Engine &en)
     DRESS_TRY(d_stats.alloc(4 * (size_t)nreq, st));
     DRESS_TRY(d_counter.alloc(1, st));
     if (ms_total > 0) DRESS_TRY(d_ms.alloc((size_t)ms_total, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(d_pdata.get(), hbytes.data(), (size_t)arena, cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(d_desc.get(), descs.data(), descs.size() * sizeof(ParentDesc),
+    DRESS_CUDA_TRY(counted_memcpy(d_pdata.get(), hbytes.data(), (size_t)arena, cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(counted_memcpy(d_desc.get(), descs.data(), descs.size() * sizeof(ParentDesc),
                                    cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(d_chunks.get(), chunks.data(), chunks.size() * sizeof(Chunk),
+    DRESS_CUDA_TRY(counted_memcpy(d_chunks.get(), chunks.data(), chunks.size() * sizeof(Chunk),
                                    cudaMemcpyHostToDevice, st));
     if (!hranks.empty())
-        DRESS_CUDA_TRY(cudaMemcpyAsync(d_ranks.get(), hranks.data(), hranks.size() * sizeof(long long),
+        DRESS_CUDA_TRY(counted_memcpy(d_ranks.get(), hranks.data(), hranks.size() * sizeof(long long),
                                        cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(cudaMemsetAsync(d_stats.get(), 0, 4 * (size_t)nreq * sizeof(unsigned long long), st));
-    DRESS_CUDA_TRY(cudaMemsetAsync(d_counter.get(), 0, sizeof(int), st));
     if (ms_total > 0) {
         // the rows of unprocessed subgraphs stay NaN, as in the reference
         size_t o = 0;
         for (Prep *p : ps)
             if (p->ms_host) {
                 size_t len = (size_t)p->total * (size_t)p->E;
-                DRESS_CUDA_TRY(cudaMemcpyAsync(d_ms.get() + o, p->ms_host, len * sizeof(double),
+                DRESS_CUDA_TRY(counted_memcpy(d_ms.get() + o, p->ms_host, len * sizeof(double),
                                                cudaMemcpyHostToDevice, st));
                 o += len;
             }
@@ -470,40 +492,81 @@ Status run_batched(std::vector<Prep *> &ps, Engine &en)
     L.edge_iters = d_stats.get() + 2 * nreq;
     L.fits = d_stats.get() + 3 * nreq;
     L.multisets = d_ms.get();
-    DRESS_TRY(launch_batch(L, en.num_sms, st));
+    P.need_hist = false;
+    for (Prep *p : ps) P.need_hist |= p->r->want_histogram != 0;
+    if (P.need_hist) DRESS_TRY(P.d_alt.alloc((size_t)values + 1, st));
+    return Status::Ok();
+}
 
-    std::vector<unsigned long long> stats(4 * (size_t)nreq);
-    DRESS_CUDA_TRY(cudaMemcpyAsync(stats.data(), d_stats.get(), stats.size() * sizeof(unsigned long long),
+// Device work of a planned batch: all fits, then the histograms (left in
+// device memory).  Can be repeated; each run starts from the same inputs.
+Status exec_batched(BatchPlan &P, Engine &en)
+{
+    cudaStream_t st = en.stream;
+    const int nreq = (int)P.ps.size();
+    DRESS_CUDA_TRY(cudaMemsetAsync(P.d_stats.get(), 0, 4 * (size_t)nreq * sizeof(unsigned long long), st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(P.d_counter.get(), 0, sizeof(int), st));
+    cudaEvent_t ev[3];
+    for (auto &e : ev) DRESS_CUDA_TRY(cudaEventCreate(&e));
+    DRESS_CUDA_TRY(cudaEventRecord(ev[0], st));
+    DRESS_TRY(launch_batch(P.L, en.num_sms, st));
+    DRESS_CUDA_TRY(cudaEventRecord(ev[1], st));
+    P.stats.assign(4 * (size_t)nreq, 0);
+    DRESS_CUDA_TRY(counted_memcpy(P.stats.data(), P.d_stats.get(), P.stats.size() * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<long long> begin((size_t)nreq), len((size_t)nreq);
-    for (int i = 0; i < nreq; ++i) {
-        begin[(size_t)i] = val_base[(size_t)i];
-        len[(size_t)i] = (long long)stats[(size_t)i];
-        ps[(size_t)i]->sweeps += stats[(size_t)nreq + i];
-        ps[(size_t)i]->edge_iters += stats[2 * (size_t)nreq + i];
-        ps[(size_t)i]->fits += stats[3 * (size_t)nreq + i];
+    if (P.need_hist) {
+        std::vector<long long> begin((size_t)nreq), len((size_t)nreq);
+        for (int i = 0; i < nreq; ++i) {
+            begin[(size_t)i] = P.val_base[(size_t)i];
+            len[(size_t)i] = (long long)P.stats[(size_t)i];
+        }
+        DRESS_TRY(histogram_device(P.d_vals.get(), P.d_alt.get(), begin, len, P.hist, st, en.num_sms));
     }
-    bool need_hist = false;
-    for (Prep *p : ps) need_hist |= p->r->want_histogram != 0;
-    if (need_hist) {
-        DRESS_TRY(d_alt.alloc((size_t)values + 1, st));
+    DRESS_CUDA_TRY(cudaEventRecord(ev[2], st));
+    DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&P.fit_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&P.hist_ms, ev[1], ev[2]);
+    for (auto &e : ev) cudaEventDestroy(e);
+    return Status::Ok();
+}
+
+// Results of the last run into the requests' host-side state.
+Status collect_batched(BatchPlan &P, Engine &en)
+{
+    cudaStream_t st = en.stream;
+    const int nreq = (int)P.ps.size();
+    std::vector<Prep *> &ps = P.ps;
+    for (int i = 0; i < nreq; ++i) {
+        ps[(size_t)i]->sweeps = P.stats[(size_t)nreq + i];
+        ps[(size_t)i]->edge_iters = P.stats[2 * (size_t)nreq + i];
+        ps[(size_t)i]->fits = P.stats[3 * (size_t)nreq + i];
+    }
+    if (P.need_hist) {
         std::vector<std::vector<long long>> out;
-        DRESS_TRY(histogram_segments(d_vals.get(), d_alt.get(), begin, len, out, st, en.num_sms));
+        DRESS_TRY(histogram_download(P.hist, out, st));
         for (int i = 0; i < nreq; ++i) ps[(size_t)i]->hist = std::move(out[(size_t)i]);
     }
-    if (ms_total > 0) {
+    if (P.ms_total > 0) {
         size_t o = 0;
         for (Prep *p : ps)
             if (p->ms_host) {
                 size_t n = (size_t)p->total * (size_t)p->E;
-                DRESS_CUDA_TRY(cudaMemcpyAsync(p->ms_host, d_ms.get() + o, n * sizeof(double),
+                DRESS_CUDA_TRY(counted_memcpy(p->ms_host, P.d_ms.get() + o, n * sizeof(double),
                                                cudaMemcpyDeviceToHost, st));
                 o += n;
             }
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     }
     return Status::Ok();
+}
+
+Status run_batched(std::vector<Prep *> &ps, Engine &en)
+{
+    BatchPlan P;
+    DRESS_TRY(plan_batched(ps, en, P));
+    DRESS_TRY(exec_batched(P, en));
+    return collect_batched(P, en);
 }
 
 Status finish(Prep &p)
@@ -735,6 +798,139 @@ dress_hist_pair_t *dress_nabla_fit_cuda(p_dress_graph_t g, int k, int iterations
 {
     return dress_nabla_fit_cuda_strided(g, k, iterations, epsilon, n_samples, seed, hist_size, keep_multisets,
                                         multisets, num_tuples, 0, 1);
+}
+
+}  // extern "C"
+
+// ---- prepared batches ------------------------------------------------------------------
+struct dressx_batch {
+    std::vector<dress::Prep> preps;
+    std::vector<dress::Prep *> ptrs;
+    dress::BatchPlan plan;
+    bool ran = false;
+};
+
+namespace dress {
+namespace {
+Status batch_create(dressx_hist_request_t *reqs, int n, dressx_batch_t **out)
+{
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    DRESS_TRY(en.init());
+    DRESS_CUDA_TRY(cudaSetDevice(en.device));
+    dressx_batch_t *b = new dressx_batch_t();
+    b->preps.resize((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        Prep &p = b->preps[(size_t)i];
+        p.r = &reqs[i];
+        reqs[i].status = DRESSX_OK;
+        reqs[i].hist_flat = nullptr;
+        reqs[i].hist_len = 0;
+        reqs[i].multisets = nullptr;
+        Status s = prepare(p);
+        if (s.ok() && (p.inplace || (!p.empty && !p.batchable)))
+            s = Status::Err(DRESSX_EUNSUPPORTED, "request needs the per-subgraph or in-place path");
+        if (!s.ok()) {
+            for (auto &q : b->preps) std::free(q.ms_host);
+            delete b;
+            return s;
+        }
+        if (!p.empty) b->ptrs.push_back(&p);
+    }
+    if (!b->ptrs.empty()) {
+        Status s = plan_batched(b->ptrs, en, b->plan);
+        if (!s.ok()) {
+            for (auto &q : b->preps) std::free(q.ms_host);
+            delete b;
+            return s;
+        }
+    }
+    *out = b;
+    return Status::Ok();
+}
+}  // namespace
+}  // namespace dress
+
+extern "C" {
+
+int dressx_batch_create(dressx_hist_request_t *reqs, int n, dressx_batch_t **out)
+{
+    if (!reqs || n < 0 || !out) return DRESSX_EINVAL;
+    *out = nullptr;
+    Status s = batch_create(reqs, n, out);
+    set_last_error(s);
+    return s.code;
+}
+
+int dressx_batch_run(dressx_batch_t *b)
+{
+    if (!b) return DRESSX_EINVAL;
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    Status s = b->ptrs.empty() ? Status::Ok() : exec_batched(b->plan, en);
+    b->ran = s.ok();
+    set_last_error(s);
+    return s.code;
+}
+
+int dressx_batch_fetch(dressx_batch_t *b)
+{
+    if (!b || !b->ran) return DRESSX_EINVAL;
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    Status s = b->ptrs.empty() ? Status::Ok() : collect_batched(b->plan, en);
+    for (auto &p : b->preps) {
+        if (!s.ok()) break;
+        std::free(p.r->hist_flat);
+        p.r->hist_flat = nullptr;
+        std::free(p.r->multisets);
+        p.r->multisets = nullptr;
+        double *ms = p.ms_host;
+        if (ms) {
+            // hand the caller a copy so the batch can be fetched again
+            size_t len = (size_t)p.total * (size_t)p.E;
+            p.ms_host = (double *)std::malloc((len ? len : 1) * sizeof(double));
+            if (p.ms_host) std::memcpy(p.ms_host, ms, len * sizeof(double));
+        }
+        s = finish(p);
+        p.ms_host = ms;
+    }
+    set_last_error(s);
+    return s.code;
+}
+
+int dressx_batch_stats(dressx_batch_t *b, int64_t *fits, int64_t *sweeps, int64_t *edge_updates)
+{
+    if (!b || !b->ran) return DRESSX_EINVAL;
+    long long f = 0, sw = 0, eu = 0;
+    const size_t n = b->ptrs.size();
+    for (size_t i = 0; i < n && b->plan.stats.size() >= 4 * n; ++i) {
+        sw += (long long)b->plan.stats[n + i];
+        eu += (long long)b->plan.stats[2 * n + i];
+        f += (long long)b->plan.stats[3 * n + i];
+    }
+    if (fits) *fits = f;
+    if (sweeps) *sweeps = sw;
+    if (edge_updates) *edge_updates = eu;
+    return DRESSX_OK;
+}
+
+int dressx_batch_timing(dressx_batch_t *b, double *fit_ms, double *hist_ms)
+{
+    if (!b || !b->ran) return DRESSX_EINVAL;
+    if (fit_ms) *fit_ms = b->plan.fit_ms;
+    if (hist_ms) *hist_ms = b->plan.hist_ms;
+    return DRESSX_OK;
+}
+
+void dressx_batch_destroy(dressx_batch_t *b)
+{
+    if (!b) return;
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    for (auto &p : b->preps) std::free(p.ms_host);
+    delete b;
+    cudaStreamSynchronize(en.stream);
 }
 
 }  // extern "C"

@@ -143,4 +143,26 @@ void dress_fit(p_dress_graph_t g, int max_iterations, double epsilon, int *itera
 
 void dressx_free(void *p) { free(p); }
 
+int dressx_stream(void **stream)
+{
+    if (!stream) return DRESSX_EINVAL;
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    Status s = en.init();
+    set_last_error(s);
+    *stream = s.ok() ? (void *)en.stream : nullptr;
+    return s.code;
+}
+
+int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, int reset)
+{
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    if (h2d_bytes) *h2d_bytes = en.h2d_bytes;
+    if (d2h_bytes) *d2h_bytes = en.d2h_bytes;
+    if (launches) *launches = en.launches;
+    if (reset) en.h2d_bytes = en.d2h_bytes = en.launches = 0;
+    return DRESSX_OK;
+}
+
 }  // extern "C"

@@ -97,11 +97,25 @@ struct Engine {
     Pinned pinned;
     int num_sms = 148;
     dressx_config_t cfg;
+    // traffic and launch counters of the public calls (reset by the caller)
+    long long h2d_bytes = 0, d2h_bytes = 0, launches = 0;
     Status init();
 };
 
 Engine &engine();
 void set_last_error(const Status &s);
+
+inline void count_h2d(size_t b) { engine().h2d_bytes += (long long)b; }
+inline void count_d2h(size_t b) { engine().d2h_bytes += (long long)b; }
+inline void count_launch(int n = 1) { engine().launches += n; }
+
+// cudaMemcpyAsync that also counts the bytes it moves between host and device
+inline cudaError_t counted_memcpy(void *dst, const void *src, size_t n, cudaMemcpyKind kind, cudaStream_t st)
+{
+    if (kind == cudaMemcpyHostToDevice) count_h2d(n);
+    else if (kind == cudaMemcpyDeviceToHost) count_d2h(n);
+    return cudaMemcpyAsync(dst, src, n, kind, st);
+}
 
 // ---- device utilities (scan.cu) -------------------------------------------
 // out[i] = sum_{j<i} in[i] for i in [0, n], out[n] = total.  `tmp` must hold

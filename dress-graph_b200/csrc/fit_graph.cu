@@ -294,6 +294,11 @@ __global__ void k_new_pairs(int E, const int *eperm, const long long *ioff_old, 
     }
 }
 
+__global__ void k_fill(int n, double v, double *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = v;
+}
+
 __global__ void k_unpermute(int n, const int *perm, const double *src, double *dst)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -516,34 +521,34 @@ Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, int sms, int
     // hub items first: they carry the longest sequential sums
     if (vb.start[BBLOCK + 1] > vb.start[BBLOCK]) {
         int n = vb.start[BBLOCK + 1] - vb.start[BBLOCK];
-        k_vertex_block<UNIF><<<grid_for(n, 1, 2 * sms), 512, (size_t)block_cap * 8, st>>>(
+        count_launch(), k_vertex_block<UNIF><<<grid_for(n, 1, 2 * sms), 512, (size_t)block_cap * 8, st>>>(
             s, vb.start[BBLOCK], vb.start[BBLOCK + 1], block_cap);
     }
     if (vb.start[BWARP + 1] > vb.start[BWARP]) {
         int n = vb.start[BWARP + 1] - vb.start[BWARP];
-        k_vertex_warp<UNIF><<<grid_for(n, 8, 8 * sms), 256, 8 * WARP_CAP * 8, st>>>(
+        count_launch(), k_vertex_warp<UNIF><<<grid_for(n, 8, 8 * sms), 256, 8 * WARP_CAP * 8, st>>>(
             s, vb.start[BWARP], vb.start[BWARP + 1]);
     }
 #define DRESS_VTHR(BIN, M)                                                                   \
     if (vb.start[BIN + 1] > vb.start[BIN])                                                   \
-        k_vertex_thr<M, UNIF><<<grid_for(vb.start[BIN + 1] - vb.start[BIN], T, INT_MAX), T, 0, st>>>( \
+        count_launch(), k_vertex_thr<M, UNIF><<<grid_for(vb.start[BIN + 1] - vb.start[BIN], T, INT_MAX), T, 0, st>>>( \
             s, vb.start[BIN], vb.start[BIN + 1]);
     DRESS_VTHR(B32, 32) DRESS_VTHR(B16, 16) DRESS_VTHR(B8, 8) DRESS_VTHR(B4, 4) DRESS_VTHR(B2, 2)
     DRESS_VTHR(B1, 1)
 #undef DRESS_VTHR
     if (eb.start[BBLOCK + 1] > eb.start[BBLOCK]) {
         int n = eb.start[BBLOCK + 1] - eb.start[BBLOCK];
-        k_edge_block<UNIF><<<grid_for(n, 1, 2 * sms), 512, (size_t)block_cap * 8, st>>>(
+        count_launch(), k_edge_block<UNIF><<<grid_for(n, 1, 2 * sms), 512, (size_t)block_cap * 8, st>>>(
             s, eb.start[BBLOCK], eb.start[BBLOCK + 1], block_cap);
     }
     if (eb.start[BWARP + 1] > eb.start[BWARP]) {
         int n = eb.start[BWARP + 1] - eb.start[BWARP];
-        k_edge_warp<UNIF><<<grid_for(n, 8, 8 * sms), 256, 8 * WARP_CAP * 8, st>>>(
+        count_launch(), k_edge_warp<UNIF><<<grid_for(n, 8, 8 * sms), 256, 8 * WARP_CAP * 8, st>>>(
             s, eb.start[BWARP], eb.start[BWARP + 1]);
     }
 #define DRESS_ETHR(BIN, M)                                                                   \
     if (eb.start[BIN + 1] > eb.start[BIN])                                                   \
-        k_edge_thr<M, UNIF><<<grid_for(eb.start[BIN + 1] - eb.start[BIN], T, INT_MAX), T, 0, st>>>( \
+        count_launch(), k_edge_thr<M, UNIF><<<grid_for(eb.start[BIN + 1] - eb.start[BIN], T, INT_MAX), T, 0, st>>>( \
             s, eb.start[BIN], eb.start[BIN + 1]);
     DRESS_ETHR(B32, 32) DRESS_ETHR(B16, 16) DRESS_ETHR(B8, 8) DRESS_ETHR(B4, 4) DRESS_ETHR(B2, 2)
     DRESS_ETHR(B1, 1)
@@ -556,7 +561,7 @@ template <class T>
 Status upload(DevBuf<T> &b, const T *host, size_t n, cudaStream_t st)
 {
     DRESS_TRY(b.alloc(n, st));
-    if (n) DRESS_CUDA_TRY(cudaMemcpyAsync(b.get(), host, n * sizeof(T), cudaMemcpyHostToDevice, st));
+    if (n) DRESS_CUDA_TRY(counted_memcpy(b.get(), host, n * sizeof(T), cudaMemcpyHostToDevice, st));
     return Status::Ok();
 }
 
@@ -578,7 +583,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         if (iterations) *iterations = max_iterations;
         return Status::Ok();
     }
-    if (N > 0 && (!g->adj_offset || !g->NW || !g->vertex_dress))
+    if (N > 0 && (!g->adj_offset || !g->vertex_dress))
         return Status::Err(DRESSX_EINVAL, "graph has NULL vertex arrays");
     if (E > 0 && (!g->U || !g->V || !g->edge_weight || !g->edge_dress || !g->adj_target ||
                   !g->adj_edge_idx))
@@ -601,7 +606,12 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(upload(d_V, g->V, (size_t)E, st));
     DRESS_TRY(upload(d_w, g->edge_weight, (size_t)E, st));
     DRESS_TRY(upload(d_d, g->edge_dress, (size_t)E, st));
-    DRESS_TRY(upload(d_nw, g->NW, (size_t)N, st));
+    if (g->NW) {
+        DRESS_TRY(upload(d_nw, g->NW, (size_t)N, st));
+    } else {                                   // NULL vertex weights mean all 1.0
+        DRESS_TRY(d_nw.alloc((size_t)N, st));
+        if (N) count_launch(), k_fill<<<grid_for(N, 256, 16 * sms), 256, 0, st>>>(N, 1.0, d_nw.get());
+    }
 
     // ---- validate ----------------------------------------------------------
     DevBuf<int> d_flags, d_deg, d_cnt;
@@ -609,13 +619,13 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_deg.alloc((size_t)N, st));
     DRESS_TRY(d_cnt.alloc((size_t)E, st));
     DRESS_CUDA_TRY(cudaMemsetAsync(d_flags.get(), 0, 8 * sizeof(int), st));
-    k_validate_rows<<<grid_for(N, 256, 16 * sms), 256, 0, st>>>(N, E, d_off.get(), d_tgt.get(),
+    count_launch(), k_validate_rows<<<grid_for(N, 256, 16 * sms), 256, 0, st>>>(N, E, d_off.get(), d_tgt.get(),
                                                                 d_eidx.get(), d_deg.get(), d_flags.get());
-    k_validate_edges<<<grid_for(E, 256, 16 * sms), 256, 0, st>>>(N, E, d_U.get(), d_V.get(), d_w.get(),
+    count_launch(), k_validate_edges<<<grid_for(E, 256, 16 * sms), 256, 0, st>>>(N, E, d_U.get(), d_V.get(), d_w.get(),
                                                                  d_flags.get());
     DRESS_CUDA_TRY(cudaGetLastError());
     int flags[8];
-    DRESS_CUDA_TRY(cudaMemcpyAsync(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     if (flags[0]) return Status::Err(DRESSX_EINVAL, "malformed graph (CSR or edge endpoints out of range)");
     const bool dup = flags[1] != 0;
@@ -637,12 +647,12 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         if (Tg < 0) return Status::Err(DRESSX_EINVAL, "bad intercept_offset");
         DRESS_TRY(upload(d_ux, g->intercept_edge_ux, (size_t)Tg, st));
         DRESS_TRY(upload(d_vx, g->intercept_edge_vx, (size_t)Tg, st));
-        k_given_counts<<<eg, 256, 0, st>>>(E, d_io.get(), d_cnt.get(), d_flags.get());
+        count_launch(), k_given_counts<<<eg, 256, 0, st>>>(E, d_io.get(), d_cnt.get(), d_flags.get());
         DRESS_TRY(exclusive_scan_i32(d_cnt.get(), d_ioff_old.get(), E, d_scan_tmp.get(), st));
-        DRESS_CUDA_TRY(cudaMemcpyAsync(&T, d_ioff_old.get() + E, sizeof(T), cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(counted_memcpy(&T, d_ioff_old.get() + E, sizeof(T), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         DRESS_TRY(d_pairs_old.alloc((size_t)(T > 0 ? T : 1), st));
-        k_given_pairs<<<eg, 256, 0, st>>>(E, d_io.get(), d_ux.get(), d_vx.get(), d_ioff_old.get(),
+        count_launch(), k_given_pairs<<<eg, 256, 0, st>>>(E, d_io.get(), d_ux.get(), d_vx.get(), d_ioff_old.get(),
                                           d_pairs_old.get(), d_flags.get());
     } else if (g->variant == DRESS_VARIANT_UNDIRECTED && !dup) {
         DevBuf<int> d_ocnt, d_otgt, d_oeid, d_osrc;
@@ -654,33 +664,33 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         DRESS_TRY(d_oeid.alloc((size_t)(S > 0 ? S : 1), st));
         DRESS_TRY(d_osrc.alloc((size_t)(S > 0 ? S : 1), st));
         const int vg = (int)grid_for(N, 256, 32 * sms);
-        k_orient_count<<<vg, 256, 0, st>>>(N, d_off.get(), d_tgt.get(), d_deg.get(), d_ocnt.get());
+        count_launch(), k_orient_count<<<vg, 256, 0, st>>>(N, d_off.get(), d_tgt.get(), d_deg.get(), d_ocnt.get());
         DRESS_TRY(exclusive_scan_i32(d_ocnt.get(), d_ooff.get(), N, d_scan_tmp.get(), st));
-        k_orient_fill<<<vg, 256, 0, st>>>(N, d_off.get(), d_tgt.get(), d_eidx.get(), d_deg.get(),
+        count_launch(), k_orient_fill<<<vg, 256, 0, st>>>(N, d_off.get(), d_tgt.get(), d_eidx.get(), d_deg.get(),
                                           d_ooff.get(), d_otgt.get(), d_oeid.get(), d_osrc.get());
         long long M = 0;
-        DRESS_CUDA_TRY(cudaMemcpyAsync(&M, d_ooff.get() + N, sizeof(M), cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(counted_memcpy(&M, d_ooff.get() + N, sizeof(M), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaMemsetAsync(d_cnt.get(), 0, (size_t)E * sizeof(int), st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         const int tg = (int)grid_for(M, 256, 64 * sms);
-        k_triangles<false><<<tg, 256, 0, st>>>(M, d_ooff.get(), d_otgt.get(), d_oeid.get(), d_osrc.get(),
+        count_launch(), k_triangles<false><<<tg, 256, 0, st>>>(M, d_ooff.get(), d_otgt.get(), d_oeid.get(), d_osrc.get(),
                                                d_cnt.get(), nullptr, nullptr);
         DRESS_TRY(exclusive_scan_i32(d_cnt.get(), d_ioff_old.get(), E, d_scan_tmp.get(), st));
-        DRESS_CUDA_TRY(cudaMemcpyAsync(&T, d_ioff_old.get() + E, sizeof(T), cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(counted_memcpy(&T, d_ioff_old.get() + E, sizeof(T), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         DRESS_TRY(d_pairs_old.alloc((size_t)(T > 0 ? T : 1), st));
         DRESS_TRY(d_cursor.alloc((size_t)E, st));
-        k_copy_i64<<<eg, 256, 0, st>>>(E, d_ioff_old.get(), d_cursor.get());
-        k_triangles<true><<<tg, 256, 0, st>>>(M, d_ooff.get(), d_otgt.get(), d_oeid.get(), d_osrc.get(),
+        count_launch(), k_copy_i64<<<eg, 256, 0, st>>>(E, d_ioff_old.get(), d_cursor.get());
+        count_launch(), k_triangles<true><<<tg, 256, 0, st>>>(M, d_ooff.get(), d_otgt.get(), d_oeid.get(), d_osrc.get(),
                                               nullptr, d_cursor.get(), d_pairs_old.get());
     } else {
-        k_merge_intercepts<false><<<eg, 256, 0, st>>>(E, d_U.get(), d_V.get(), d_off.get(), d_tgt.get(),
+        count_launch(), k_merge_intercepts<false><<<eg, 256, 0, st>>>(E, d_U.get(), d_V.get(), d_off.get(), d_tgt.get(),
                                                        d_eidx.get(), d_cnt.get(), nullptr, nullptr);
         DRESS_TRY(exclusive_scan_i32(d_cnt.get(), d_ioff_old.get(), E, d_scan_tmp.get(), st));
-        DRESS_CUDA_TRY(cudaMemcpyAsync(&T, d_ioff_old.get() + E, sizeof(T), cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(counted_memcpy(&T, d_ioff_old.get() + E, sizeof(T), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         DRESS_TRY(d_pairs_old.alloc((size_t)(T > 0 ? T : 1), st));
-        k_merge_intercepts<true><<<eg, 256, 0, st>>>(E, d_U.get(), d_V.get(), d_off.get(), d_tgt.get(),
+        count_launch(), k_merge_intercepts<true><<<eg, 256, 0, st>>>(E, d_U.get(), d_V.get(), d_off.get(), d_tgt.get(),
                                                       d_eidx.get(), nullptr, d_ioff_old.get(),
                                                       d_pairs_old.get());
     }
@@ -696,11 +706,11 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_einv.alloc((size_t)E, st));
     DRESS_CUDA_TRY(cudaMemsetAsync(d_bc.get(), 0, 4 * NB * sizeof(int), st));
     const int vg = (int)grid_for(N, 256, 32 * sms);
-    k_bin_count<<<vg, 256, 0, st>>>(N, d_deg.get(), 1, d_bc.get());
-    k_bin_count<<<eg, 256, 0, st>>>(E, d_cnt.get(), 1, d_bc.get() + NB);
+    count_launch(), k_bin_count<<<vg, 256, 0, st>>>(N, d_deg.get(), 1, d_bc.get());
+    count_launch(), k_bin_count<<<eg, 256, 0, st>>>(E, d_cnt.get(), 1, d_bc.get() + NB);
     int bc[2 * NB];
-    DRESS_CUDA_TRY(cudaMemcpyAsync(bc, d_bc.get(), sizeof(bc), cudaMemcpyDeviceToHost, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(counted_memcpy(bc, d_bc.get(), sizeof(bc), cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     if (flags[0]) return Status::Err(DRESSX_EINVAL, "malformed intercept tables");
     Bins vb, eb;
@@ -711,9 +721,9 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     }
     int cur[2 * NB];
     for (int b = 0; b < NB; ++b) { cur[b] = vb.start[b]; cur[NB + b] = eb.start[b]; }
-    DRESS_CUDA_TRY(cudaMemcpyAsync(d_bc.get() + 2 * NB, cur, sizeof(cur), cudaMemcpyHostToDevice, st));
-    k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), 1, d_bc.get() + 2 * NB, d_vperm.get(), d_vinv.get());
-    k_bin_scatter<<<eg, 256, 0, st>>>(E, d_cnt.get(), 1, d_bc.get() + 3 * NB, d_eperm.get(), d_einv.get());
+    DRESS_CUDA_TRY(counted_memcpy(d_bc.get() + 2 * NB, cur, sizeof(cur), cudaMemcpyHostToDevice, st));
+    count_launch(), k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), 1, d_bc.get() + 2 * NB, d_vperm.get(), d_vinv.get());
+    count_launch(), k_bin_scatter<<<eg, 256, 0, st>>>(E, d_cnt.get(), 1, d_bc.get() + 3 * NB, d_eperm.get(), d_einv.get());
 
     DevBuf<int> d_ndeg, d_row_eid, d_eu, d_ev, d_ncnt;
     DevBuf<long long> d_row_off, d_ioff;
@@ -723,9 +733,9 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_row_off.alloc((size_t)N + 1, st));
     DRESS_TRY(d_row_eid.alloc((size_t)(S > 0 ? S : 1), st));
     DRESS_TRY(d_nwi.alloc((size_t)N, st));
-    k_gather_deg<<<vg, 256, 0, st>>>(N, d_vperm.get(), d_deg.get(), d_ndeg.get());
+    count_launch(), k_gather_deg<<<vg, 256, 0, st>>>(N, d_vperm.get(), d_deg.get(), d_ndeg.get());
     DRESS_TRY(exclusive_scan_i32(d_ndeg.get(), d_row_off.get(), N, d_scan_tmp.get(), st));
-    k_new_rows<<<grid_for((long long)N * 32, 256, 64 * sms), 256, 0, st>>>(
+    count_launch(), k_new_rows<<<grid_for((long long)N * 32, 256, 64 * sms), 256, 0, st>>>(
         N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(), d_row_off.get(), d_row_eid.get(),
         d_nw.get(), d_nwi.get());
     d_eidx.release();
@@ -739,14 +749,14 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         DRESS_TRY(d_wi.alloc((size_t)E, st));
         DRESS_TRY(d_pbuf.alloc(2 * (size_t)E, st));
     }
-    k_new_edges<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_U.get(), d_V.get(), d_vinv.get(), d_w.get(),
+    count_launch(), k_new_edges<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_U.get(), d_V.get(), d_vinv.get(), d_w.get(),
                                     d_d.get(), d_cnt.get(), d_eu.get(), d_ev.get(),
                                     uniform ? nullptr : d_wi.get(), d_dbuf.get(),
                                     uniform ? nullptr : d_pbuf.get(), d_ncnt.get());
     DRESS_TRY(d_ioff.alloc((size_t)E + 1, st));
     DRESS_TRY(exclusive_scan_i32(d_ncnt.get(), d_ioff.get(), E, d_scan_tmp.get(), st));
     DRESS_TRY(d_pairs.alloc((size_t)(T > 0 ? T : 1), st));
-    k_new_pairs<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_ioff_old.get(), d_pairs_old.get(), d_einv.get(),
+    count_launch(), k_new_pairs<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_ioff_old.get(), d_pairs_old.get(), d_einv.get(),
                                     d_ioff.get(), d_pairs.get());
     DRESS_CUDA_TRY(cudaGetLastError());
     d_U.release(); d_V.release(); d_w.release(); d_d.release(); d_nw.release();
@@ -780,7 +790,10 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_maxd.alloc(RING, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     double setup_ms = ms_since(t0);
-    auto t1 = std::chrono::steady_clock::now();
+    cudaEvent_t sw0, sw1;
+    DRESS_CUDA_TRY(cudaEventCreate(&sw0));
+    DRESS_CUDA_TRY(cudaEventCreate(&sw1));
+    DRESS_CUDA_TRY(cudaEventRecord(sw0, st));
 
     // ---- sweeps -------------------------------------------------------------
     Sweep s;
@@ -816,7 +829,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
             if (uniform) DRESS_TRY(launch_sweep<true>(s, vb, eb, sms, block_cap, st));
             else         DRESS_TRY(launch_sweep<false>(s, vb, eb, sms, block_cap, st));
         }
-        DRESS_CUDA_TRY(cudaMemcpyAsync(hmax, d_maxd.get(), RING * sizeof(unsigned long long),
+        DRESS_CUDA_TRY(counted_memcpy(hmax, d_maxd.get(), RING * sizeof(unsigned long long),
                                        cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         for (int it = done; it < hi; ++it) {
@@ -829,17 +842,24 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         if (chunk < 32) chunk *= 2;
     }
     const int last = conv >= 0 ? conv : max_iterations - 1;
+    // device time of the sweeps (the chunk tails after convergence return at once)
+    DRESS_CUDA_TRY(cudaEventRecord(sw1, st));
+    DRESS_CUDA_TRY(cudaEventSynchronize(sw1));
+    float sweep_ms = 0.f;
+    cudaEventElapsedTime(&sweep_ms, sw0, sw1);
+    cudaEventDestroy(sw0);
+    cudaEventDestroy(sw1);
 
     // ---- results back in the caller's numbering ------------------------------
     DevBuf<double> d_out;
     DRESS_TRY(d_out.alloc((size_t)E + N + 1, st));
-    k_unpermute<<<eg, 256, 0, st>>>(E, d_eperm.get(), dbuf[(last + 1) & 1], d_out.get());
-    k_unpermute<<<vg, 256, 0, st>>>(N, d_vperm.get(), d_vd.get(), d_out.get() + E);
+    count_launch(), k_unpermute<<<eg, 256, 0, st>>>(E, d_eperm.get(), dbuf[(last + 1) & 1], d_out.get());
+    count_launch(), k_unpermute<<<vg, 256, 0, st>>>(N, d_vperm.get(), d_vd.get(), d_out.get() + E);
     if (E > 0)
-        DRESS_CUDA_TRY(cudaMemcpyAsync(g->edge_dress, d_out.get(), (size_t)E * sizeof(double),
+        DRESS_CUDA_TRY(counted_memcpy(g->edge_dress, d_out.get(), (size_t)E * sizeof(double),
                                        cudaMemcpyDeviceToHost, st));
     if (N > 0)
-        DRESS_CUDA_TRY(cudaMemcpyAsync(g->vertex_dress, d_out.get() + E, (size_t)N * sizeof(double),
+        DRESS_CUDA_TRY(counted_memcpy(g->vertex_dress, d_out.get() + E, (size_t)N * sizeof(double),
                                        cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     if (iterations) *iterations = conv >= 0 ? conv : max_iterations;
@@ -848,7 +868,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         stats->T = T;
         stats->sweeps = last + 1;
         stats->setup_ms = setup_ms;
-        stats->iterate_ms = ms_since(t1);
+        stats->iterate_ms = sweep_ms;
     }
     return Status::Ok();
 }

@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(HT) k_tile_scatter(const Tile *tiles, const un
     __shared__ int rtot[RADIX];
     __shared__ long long dbase[RADIX];
     Tile t = tiles[blockIdx.x];
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int wid = threadIdx.x >> 5;
     for (int d = threadIdx.x; d < RADIX; d += HT) dbase[d] = offs[(long long)blockIdx.x * RADIX + d];
     for (long long r0 = t.begin; r0 < t.end; r0 += HT) {
         for (int q = threadIdx.x; q < W * RADIX; q += HT) (&wcnt[0][0])[q] = 0;
@@ -213,12 +213,12 @@ __global__ void k_run_pairs(long long R, const long long *run_start, const unsig
 
 }  // namespace
 
-Status histogram_segments(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
-                          const std::vector<long long> &len, std::vector<std::vector<long long>> &out,
-                          cudaStream_t st, int sms)
+Status histogram_device(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
+                        const std::vector<long long> &len, HistResult &res, cudaStream_t st, int sms)
 {
     const int nseg = (int)begin.size();
-    out.assign((size_t)nseg, std::vector<long long>());
+    res.nseg = nseg;
+    res.R = 0;
     std::vector<Tile> tiles;
     std::vector<int> seg_tile0((size_t)nseg + 1, 0);
     std::vector<long long> seg_end((size_t)nseg);
@@ -239,8 +239,8 @@ Status histogram_segments(unsigned long long *keys, unsigned long long *alt, con
     const int nt = (int)tiles.size();
 
     DevBuf<Tile> d_tiles;
-    DevBuf<int> d_seg_tile0, d_counts, d_moves, d_run_seg;
-    DevBuf<long long> d_seg_begin, d_seg_end, d_offs, d_tile_heads, d_tile_base, d_scan_tmp, d_run_start, d_pairs;
+    DevBuf<int> d_seg_tile0, d_counts, d_moves;
+    DevBuf<long long> d_seg_begin, d_seg_end, d_offs, d_tile_heads, d_tile_base, d_scan_tmp, d_run_start;
     DevBuf<unsigned long long> d_run_bits;
     DRESS_TRY(d_tiles.alloc((size_t)nt, st));
     DRESS_TRY(d_seg_tile0.alloc((size_t)nseg + 1, st));
@@ -249,29 +249,29 @@ Status histogram_segments(unsigned long long *keys, unsigned long long *alt, con
     DRESS_TRY(d_counts.alloc((size_t)nt * RADIX, st));
     DRESS_TRY(d_offs.alloc((size_t)nt * RADIX, st));
     DRESS_TRY(d_moves.alloc(1, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(d_tiles.get(), tiles.data(), (size_t)nt * sizeof(Tile), cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(d_seg_tile0.get(), seg_tile0.data(), ((size_t)nseg + 1) * sizeof(int),
+    DRESS_CUDA_TRY(counted_memcpy(d_tiles.get(), tiles.data(), (size_t)nt * sizeof(Tile), cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(counted_memcpy(d_seg_tile0.get(), seg_tile0.data(), ((size_t)nseg + 1) * sizeof(int),
                                    cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(d_seg_begin.get(), begin.data(), (size_t)nseg * sizeof(long long),
+    DRESS_CUDA_TRY(counted_memcpy(d_seg_begin.get(), begin.data(), (size_t)nseg * sizeof(long long),
                                    cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(d_seg_end.get(), seg_end.data(), (size_t)nseg * sizeof(long long),
+    DRESS_CUDA_TRY(counted_memcpy(d_seg_end.get(), seg_end.data(), (size_t)nseg * sizeof(long long),
                                    cudaMemcpyHostToDevice, st));
 
     // order-preserving image of the doubles over the used span
-    k_to_ordered<<<(unsigned)((hi - lo + 255) / 256 < 64 * sms ? (hi - lo + 255) / 256 : 64 * sms), 256, 0, st>>>(
+    count_launch(), k_to_ordered<<<(unsigned)((hi - lo + 255) / 256 < 64 * sms ? (hi - lo + 255) / 256 : 64 * sms), 256, 0, st>>>(
         hi - lo, keys + lo);
     unsigned long long *a = keys, *b = alt;
     for (int pass = 0; pass < 8; ++pass) {
         int shift = 8 * pass;
-        k_tile_hist<<<nt, HT, 0, st>>>(d_tiles.get(), a, shift, d_counts.get());
+        count_launch(), k_tile_hist<<<nt, HT, 0, st>>>(d_tiles.get(), a, shift, d_counts.get());
         DRESS_CUDA_TRY(cudaMemsetAsync(d_moves.get(), 0, sizeof(int), st));
-        k_seg_offsets<<<nseg, RADIX, 0, st>>>(d_seg_begin.get(), d_seg_tile0.get(), d_counts.get(), d_offs.get(),
+        count_launch(), k_seg_offsets<<<nseg, RADIX, 0, st>>>(d_seg_begin.get(), d_seg_tile0.get(), d_counts.get(), d_offs.get(),
                                               d_moves.get());
         int moves = 0;
-        DRESS_CUDA_TRY(cudaMemcpyAsync(&moves, d_moves.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(counted_memcpy(&moves, d_moves.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         if (!moves) continue;
-        k_tile_scatter<<<nt, HT, 0, st>>>(d_tiles.get(), a, b, shift, d_offs.get());
+        count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(d_tiles.get(), a, b, shift, d_offs.get());
         unsigned long long *t = a;
         a = b;
         b = t;
@@ -282,32 +282,54 @@ Status histogram_segments(unsigned long long *keys, unsigned long long *alt, con
     DRESS_TRY(d_tile_heads.alloc((size_t)nt, st));
     DRESS_TRY(d_tile_base.alloc((size_t)nt + 1, st));
     DRESS_TRY(d_scan_tmp.alloc(scan_tmp_elems(nt), st));
-    k_tile_heads<<<nt, HT, 0, st>>>(d_tiles.get(), d_seg_begin.get(), a, d_tile_heads.get());
+    count_launch(), k_tile_heads<<<nt, HT, 0, st>>>(d_tiles.get(), d_seg_begin.get(), a, d_tile_heads.get());
     DRESS_TRY(exclusive_scan_i64(d_tile_heads.get(), d_tile_base.get(), nt, d_scan_tmp.get(), st));
     long long R = 0;
-    DRESS_CUDA_TRY(cudaMemcpyAsync(&R, d_tile_base.get() + nt, sizeof(R), cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(counted_memcpy(&R, d_tile_base.get() + nt, sizeof(R), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     DRESS_TRY(d_run_start.alloc((size_t)R, st));
     DRESS_TRY(d_run_bits.alloc((size_t)R, st));
-    DRESS_TRY(d_run_seg.alloc((size_t)R, st));
-    DRESS_TRY(d_pairs.alloc(2 * (size_t)R, st));
-    k_tile_runs<<<nt, HT, 0, st>>>(d_tiles.get(), d_seg_begin.get(), a, d_tile_base.get(), d_run_start.get(),
-                                   d_run_bits.get(), d_run_seg.get());
-    k_run_pairs<<<(unsigned)((R + 255) / 256 < 64 * sms ? (R + 255) / 256 : 64 * sms), 256, 0, st>>>(
-        R, d_run_start.get(), d_run_bits.get(), d_run_seg.get(), d_seg_end.get(), d_pairs.get());
+    DRESS_TRY(res.run_seg.alloc((size_t)R, st));
+    DRESS_TRY(res.pairs.alloc(2 * (size_t)R, st));
+    count_launch(), k_tile_runs<<<nt, HT, 0, st>>>(d_tiles.get(), d_seg_begin.get(), a, d_tile_base.get(), d_run_start.get(),
+                                   d_run_bits.get(), res.run_seg.get());
+    count_launch(), k_run_pairs<<<(unsigned)((R + 255) / 256 < 64 * sms ? (R + 255) / 256 : 64 * sms), 256, 0, st>>>(
+        R, d_run_start.get(), d_run_bits.get(), res.run_seg.get(), d_seg_end.get(), res.pairs.get());
     DRESS_CUDA_TRY(cudaGetLastError());
+    res.R = R;
+    return Status::Ok();
+}
+
+Status histogram_download(HistResult &res, std::vector<std::vector<long long>> &out, cudaStream_t st)
+{
+    out.assign((size_t)res.nseg, std::vector<long long>());
+    const long long R = res.R;
+    if (R == 0) return Status::Ok();
     std::vector<long long> pairs(2 * (size_t)R);
     std::vector<int> rseg((size_t)R);
-    DRESS_CUDA_TRY(cudaMemcpyAsync(pairs.data(), d_pairs.get(), 2 * (size_t)R * sizeof(long long),
+    DRESS_CUDA_TRY(counted_memcpy(pairs.data(), res.pairs.get(), 2 * (size_t)R * sizeof(long long),
                                    cudaMemcpyDeviceToHost, st));
-    DRESS_CUDA_TRY(cudaMemcpyAsync(rseg.data(), d_run_seg.get(), (size_t)R * sizeof(int), cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(counted_memcpy(rseg.data(), res.run_seg.get(), (size_t)R * sizeof(int), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-    for (long long r = 0; r < R; ++r) {
-        auto &v = out[(size_t)rseg[(size_t)r]];
-        v.push_back(pairs[2 * (size_t)r]);
-        v.push_back(pairs[2 * (size_t)r + 1]);
+    // runs come out grouped by segment, in segment order
+    long long r = 0;
+    while (r < R) {
+        int sgm = rseg[(size_t)r];
+        long long e = r;
+        while (e < R && rseg[(size_t)e] == sgm) ++e;
+        out[(size_t)sgm].assign(pairs.begin() + 2 * r, pairs.begin() + 2 * e);
+        r = e;
     }
     return Status::Ok();
+}
+
+Status histogram_segments(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
+                          const std::vector<long long> &len, std::vector<std::vector<long long>> &out,
+                          cudaStream_t st, int sms)
+{
+    HistResult res;
+    DRESS_TRY(histogram_device(keys, alt, begin, len, res, st, sms));
+    return histogram_download(res, out, st);
 }
 
 }  // namespace dress

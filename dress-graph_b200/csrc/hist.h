@@ -6,6 +6,20 @@
 
 namespace dress {
 
+// Histogram runs left in device memory: pairs[2r], pairs[2r+1] = (value
+// bits, count) of run r; run_seg[r] = its segment; runs are grouped by
+// segment in segment order.
+struct HistResult {
+    DevBuf<long long> pairs;
+    DevBuf<int> run_seg;
+    long long R = 0;
+    int nseg = 0;
+};
+
+Status histogram_device(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
+                        const std::vector<long long> &len, HistResult &res, cudaStream_t st, int sms);
+Status histogram_download(HistResult &res, std::vector<std::vector<long long>> &out, cudaStream_t st);
+
 // Sorts each segment [begin[s], begin[s]+len[s]) of `keys` (raw double bits)
 // and returns, per segment, the flat [value_bits, count, ...] list ascending
 // by value with ==-equal values merged.  `alt` is scratch of the same size as

@@ -103,9 +103,9 @@ Status scan_impl(const T *in, long long *out, long long n, long long *tmp, cudaS
         return Status::Ok();
     }
     long long nt = (n + TILE - 1) / TILE;
-    k_tile_sums<T><<<(unsigned)nt, SB, 0, st>>>(in, n, tmp);
-    k_scan_sums<<<1, SB, 0, st>>>(tmp, nt);
-    k_tile_scan<T><<<(unsigned)nt, SB, 0, st>>>(in, out, n, tmp);
+    count_launch(), k_tile_sums<T><<<(unsigned)nt, SB, 0, st>>>(in, n, tmp);
+    count_launch(), k_scan_sums<<<1, SB, 0, st>>>(tmp, nt);
+    count_launch(), k_tile_scan<T><<<(unsigned)nt, SB, 0, st>>>(in, out, n, tmp);
     DRESS_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
 }

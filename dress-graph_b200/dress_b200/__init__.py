@@ -275,3 +275,81 @@ def configure(device=-1, memory_budget_bytes=0, fit_chunk=0, group_threads=0):
     cfg.fit_chunk = int(fit_chunk)
     cfg.group_threads = int(group_threads)
     _check(lib().dressx_configure(ctypes.byref(cfg)))
+
+
+class Batch:
+    """A prepared batch of Delta/Nabla requests resident in device memory
+    (``dressx_batch_*``): ``run()`` re-runs every fit and histogram on the
+    device, ``fetch()`` copies the histograms back."""
+
+    def __init__(self, graphs, kind=DELTA, k=1, max_iterations=100, epsilon=1e-6, n_samples=0, seed=0,
+                 keep_multisets=False, offset=0, stride=1, compute_histogram=True):
+        self.graphs = list(graphs)
+        n = len(self.graphs)
+        self.reqs = (_abi.HistRequest * n)()
+        for i, g in enumerate(self.graphs):
+            r = self.reqs[i]
+            r.graph = g.ptr
+            r.kind, r.k = int(kind), int(k)
+            r.max_iterations, r.epsilon = int(max_iterations), float(epsilon)
+            r.n_samples, r.seed = int(n_samples), int(seed) & 0xFFFFFFFF
+            r.offset, r.stride = int(offset), int(stride)
+            r.want_histogram = 1 if compute_histogram else 0
+            r.keep_multisets = 1 if keep_multisets else 0
+        h = ctypes.c_void_p()
+        _check(lib().dressx_batch_create(self.reqs, n, ctypes.byref(h)))
+        self.handle = h
+
+    def run(self):
+        _check(lib().dressx_batch_run(self.handle))
+
+    def fetch(self):
+        _check(lib().dressx_batch_fetch(self.handle))
+        out = []
+        for i in range(len(self.graphs)):
+            r = self.reqs[i]
+            out.append(_arr(r.hist_flat, r.hist_len, np.int64))
+        return out
+
+    def stats(self):
+        f, s, e = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().dressx_batch_stats(self.handle, ctypes.byref(f), ctypes.byref(s), ctypes.byref(e)))
+        return dict(fits=f.value, sweeps=s.value, edge_updates=e.value)
+
+    def timing(self):
+        """(fit_ms, hist_ms) of the last run, CUDA events on the engine stream."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(lib().dressx_batch_timing(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if self.handle:
+            for i in range(len(self.graphs)):
+                r = self.reqs[i]
+                if r.hist_flat:
+                    lib().dressx_free(ctypes.cast(r.hist_flat, ctypes.c_void_p))
+                    r.hist_flat = None
+                if r.multisets:
+                    lib().dressx_free(ctypes.cast(r.multisets, ctypes.c_void_p))
+                    r.multisets = None
+            lib().dressx_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def stream_handle():
+    """The engine's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+    p = ctypes.c_void_p()
+    _check(lib().dressx_stream(ctypes.byref(p)))
+    return p.value or 0
+
+
+def counters(reset=False):
+    h, d, l = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    lib().dressx_counters(ctypes.byref(h), ctypes.byref(d), ctypes.byref(l), 1 if reset else 0)
+    return dict(h2d_bytes=h.value, d2h_bytes=d.value, launches=l.value)

@@ -87,6 +87,14 @@ SIGNATURES = {
     "dressx_hist_batch": (ctypes.c_int, [ctypes.POINTER(HistRequest), ctypes.c_int]),
     "dressx_hist_batch_per_fit": (ctypes.c_int, [ctypes.POINTER(HistRequest), ctypes.c_int]),
     "dressx_free": (None, [ctypes.c_void_p]),
+    "dressx_batch_create": (ctypes.c_int, [ctypes.POINTER(HistRequest), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "dressx_batch_run": (ctypes.c_int, [ctypes.c_void_p]),
+    "dressx_batch_fetch": (ctypes.c_int, [ctypes.c_void_p]),
+    "dressx_batch_stats": (ctypes.c_int, [ctypes.c_void_p, _c_i64_p, _c_i64_p, _c_i64_p]),
+    "dressx_batch_timing": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p]),
+    "dressx_batch_destroy": (None, [ctypes.c_void_p]),
+    "dressx_stream": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p)]),
+    "dressx_counters": (ctypes.c_int, [_c_i64_p, _c_i64_p, _c_i64_p, ctypes.c_int]),
 }
 
 _lib = None

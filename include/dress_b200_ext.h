@@ -56,7 +56,7 @@ typedef struct dressx_fit_stats_t {
     int64_t common_terms;      /* sum over edges of |N[u] ^ N[v]|          */
     int     sweeps;            /* sweeps executed                          */
     double  setup_ms;          /* upload + intercepts + binning            */
-    double  iterate_ms;        /* all sweeps                               */
+    double  iterate_ms;        /* all sweeps, device time (CUDA events)    */
 } dressx_fit_stats_t;
 int dressx_last_fit_stats(dressx_fit_stats_t *out);
 
@@ -89,6 +89,39 @@ typedef struct dressx_hist_request_t {
  * in the batch.  Returns the first failing status (each request also
  * carries its own). */
 int dressx_hist_batch(dressx_hist_request_t *reqs, int n);
+
+/* Same as dressx_hist_batch, but every subgraph goes through the
+ * per-subgraph path: host-built subgraph CSR + one single-graph GPU fit per
+ * subgraph, the structure of the reference driver
+ * (libdress/src/delta_dress_impl.c:268-309).  Kept as the baseline the
+ * batched engine is measured against. */
+int dressx_hist_batch_per_fit(dressx_hist_request_t *reqs, int n);
+
+/* A prepared batch: the requests' graphs packed and resident in device
+ * memory, so the fits and histograms can be re-run without host traffic.
+ * Every request must be batchable (k >= 1, rows of at most 31 neighbours);
+ * dressx_batch_create returns DRESSX_EUNSUPPORTED otherwise.  The requests
+ * must stay alive until dressx_batch_destroy. */
+typedef struct dressx_batch dressx_batch_t;
+int  dressx_batch_create(dressx_hist_request_t *reqs, int n, dressx_batch_t **out);
+/* All fits and histograms on the device; results stay in device memory. */
+int  dressx_batch_run(dressx_batch_t *b);
+/* Copies the last run's histograms (and multisets) into the requests. */
+int  dressx_batch_fetch(dressx_batch_t *b);
+/* Totals of the last run: subgraphs fitted, sweeps, live-edge updates. */
+int  dressx_batch_stats(dressx_batch_t *b, int64_t *fits, int64_t *sweeps, int64_t *edge_updates);
+/* Device time of the last run, from CUDA events on the engine stream:
+ * the batched fit kernel, and the histogram kernels after it. */
+int  dressx_batch_timing(dressx_batch_t *b, double *fit_ms, double *hist_ms);
+void dressx_batch_destroy(dressx_batch_t *b);
+
+/* The engine's CUDA stream (cudaStream_t) -- every kernel of this library
+ * is launched on it, so callers can time them with events on this stream. */
+int dressx_stream(void **stream);
+
+/* Counters since the last reset: bytes copied host->device and
+ * device->host by this library, and kernels it launched. */
+int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, int reset);
 
 /* Frees a buffer returned by this library. */
 void dressx_free(void *p);

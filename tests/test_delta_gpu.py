@@ -142,3 +142,26 @@ def test_reference_delta_test_binary():
         pytest.skip("reference test binary not built")
     out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout + out.stderr
+
+
+def test_prepared_batch_reruns_match(oracle_port):
+    """dressx_batch_*: graphs resident on the device, re-run twice, same
+    exact histograms as the one-shot call and the oracle."""
+    gs = graphs.regular_batch(12, (16, 50), (3, 9), seed=11)
+    objs = [db.Graph(n, U, V) for n, U, V in gs]
+    b = db.Batch(objs, db.DELTA, 1)
+    b.run()
+    first = b.fetch()
+    b.run()
+    second = b.fetch()
+    st = b.stats()
+    assert st["fits"] == sum(n for n, _, _ in gs)
+    fit_ms, hist_ms = b.timing()
+    assert fit_ms > 0 and hist_ms >= 0
+    for (n, U, V), x, y in zip(gs, first, second):
+        ref = oracle_port.delta_fit(n, U, V, k=1)
+        np.testing.assert_array_equal(x, ref["hist"])
+        np.testing.assert_array_equal(y, ref["hist"])
+    b.close()
+    for g in objs:
+        g.close()
