@@ -10,6 +10,8 @@
 // adjacent after the sort) and every NaN is a run of its own, as in the
 // reference's map.  A pass in which every segment has a single digit value
 // moves nothing and is skipped.
+#include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "engine.h"
@@ -333,3 +335,219 @@ Status histogram_segments(unsigned long long *keys, unsigned long long *alt, con
 }
 
 }  // namespace dress
+
+// ---------------------------------------------------------------------------
+// Histogram without any allocation (dressx_histogram_noalloc)
+//
+// Some callers cannot allocate device memory at the moment they need a
+// histogram: code running while a CUDA graph is being captured, frameworks
+// whose caching allocator owns all device memory, or real-time loops that
+// forbid allocation after start-up.  For them the pipeline above runs on one
+// segment of at most NOALLOC_MAX values with every scratch buffer carved out
+// of the file-scope array below.  Every GPU that loads this library holds the
+// array (about 16.5 MiB) until the process exits.  The call only enqueues work
+// on the caller's stream (no host synchronisation, all eight digit passes
+// always run), so results are ready when the stream reaches that point.  All
+// calls share the one array: calls whose work overlaps on the GPU race.
+// ---------------------------------------------------------------------------
+namespace dress {
+namespace {
+
+constexpr long long NOALLOC_MAX = DRESSX_NOALLOC_MAX_VALUES;
+constexpr int NA_TILES = (int)(NOALLOC_MAX / TILE);
+static_assert(NOALLOC_MAX % TILE == 0, "whole tiles");
+
+// byte offsets of the carved buffers
+constexpr long long NA_A = 0;                                       // u64 keys, sorted here
+constexpr long long NA_B = NA_A + 8 * NOALLOC_MAX;                  // u64 ping-pong / run starts
+constexpr long long NA_OFFS = NA_B + 8 * NOALLOC_MAX;               // i64 [tiles][256]
+constexpr long long NA_COUNTS = NA_OFFS + 8LL * NA_TILES * RADIX;   // i32 [tiles][256]
+constexpr long long NA_TILESB = NA_COUNTS + 4LL * NA_TILES * RADIX; // Tile [tiles]
+constexpr long long NA_HEADS = NA_TILESB + 32LL * NA_TILES;         // i64 [tiles]
+constexpr long long NA_BASE = NA_HEADS + 8LL * NA_TILES;            // i64 [tiles+1]
+constexpr long long NA_SEG = NA_BASE + 8LL * (NA_TILES + 8);                          // i64 begin, i64 end, i32 tile0[2], i32 moves
+constexpr long long NA_BYTES = NA_SEG + 64;
+static_assert(sizeof(Tile) <= 32, "tile descriptor slot");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+// single segment [0, n): tile descriptors and segment bounds
+__global__ void k_na_setup(long long n, int nt, Tile *tiles, long long *seg_begin, long long *seg_end,
+                           int *seg_tile0)
+{
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        long long b = (long long)t * TILE;
+        tiles[t].begin = b;
+        tiles[t].end = b + TILE < n ? b + TILE : n;
+        tiles[t].seg = 0;
+    }
+    if (threadIdx.x == 0) {
+        seg_begin[0] = 0;
+        seg_end[0] = n;
+        seg_tile0[0] = 0;
+        seg_tile0[1] = nt;
+    }
+}
+
+__global__ void k_na_load(long long n, const double *in, unsigned long long *keys)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        keys[i] = to_ordered((unsigned long long)__double_as_longlong(in[i]));
+}
+
+// run starts into `starts`, value bits into pairs[2r]
+__global__ void __launch_bounds__(HT) k_na_runs(const Tile *tiles, const unsigned long long *keys,
+                                                const long long *tile_base, long long *starts, long long *pairs)
+{
+    __shared__ int wsum[HT / 32];
+    __shared__ long long carry;
+    Tile t = tiles[blockIdx.x];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) carry = tile_base[blockIdx.x];
+    __syncthreads();
+    for (long long r0 = t.begin; r0 < t.end; r0 += HT) {
+        long long i = r0 + threadIdx.x;
+        bool h = i < t.end && is_head(keys, i, 0);
+        unsigned b = __ballot_sync(0xffffffffu, h);
+        if (lane == 0) wsum[wid] = __popc(b);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < HT / 32; ++w) {
+            int c = wsum[w];
+            if (w < wid) before += c;
+            total += c;
+        }
+        if (h) {
+            long long r = carry + before + __popc(b & lanemask_lt_h());
+            starts[r] = i;
+            pairs[2 * r] = (long long)from_ordered(keys[i]);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += total;
+        __syncthreads();
+    }
+}
+
+// exclusive prefix of the per-tile head counts (nt <= NA_TILES values)
+__global__ void k_na_scan(const long long *heads, int nt, long long *tile_base)
+{
+    if (threadIdx.x != 0) return;
+    long long run = 0;
+    for (int t = 0; t < nt; ++t) {
+        tile_base[t] = run;
+        run += heads[t];
+    }
+    tile_base[nt] = run;
+}
+
+// counts from consecutive run starts; the run total sits at tile_base[nt]
+__global__ void k_na_counts(long long n, int nt, const long long *tile_base, const long long *starts,
+                            long long *pairs, long long *num_runs)
+{
+    const long long R = tile_base[nt];
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < R;
+         r += (long long)gridDim.x * blockDim.x) {
+        long long end = r + 1 < R ? starts[r + 1] : n;
+        pairs[2 * r + 1] = end - starts[r];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *num_runs = R;
+}
+
+}  // namespace
+}  // namespace dress
+
+namespace dress {
+namespace {
+
+constexpr int NA_MAX_DEVICES = 128;
+std::mutex g_na_mu;
+unsigned char *g_na_base[NA_MAX_DEVICES];      // device address of the array, per device
+
+// The array's name is a host-side stand-in in host code; its device address
+// comes from cudaGetSymbolAddress, once per device, with that device current.
+cudaError_t noalloc_scratch(unsigned char **out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= NA_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    if (!g_na_base[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_na_base[dev] = (unsigned char *)p;
+    }
+    *out = g_na_base[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace dress
+
+extern "C" int dressx_histogram_noalloc(const double *values, int64_t n, int64_t *pairs, int64_t *num_runs,
+                                        void *stream)
+{
+    using namespace dress;
+    if (n < 0 || (n > 0 && (!values || !pairs)) || !num_runs) {
+        std::fprintf(stderr, "dress_b200: dressx_histogram_noalloc: bad arguments\n");
+        return DRESSX_EINVAL;
+    }
+    if (n > NOALLOC_MAX) {
+        std::fprintf(stderr, "dress_b200: dressx_histogram_noalloc: %lld values exceed the maximum of %lld\n",
+                     (long long)n, (long long)NOALLOC_MAX);
+        return DRESSX_EUNSUPPORTED;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned char *base = nullptr;
+    cudaError_t e = noalloc_scratch(&base);
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "dress_b200: dressx_histogram_noalloc: scratch address: %s\n", cudaGetErrorString(e));
+        return DRESSX_ECUDA;
+    }
+    if (n == 0) {
+        e = cudaMemsetAsync(num_runs, 0, sizeof(int64_t), st);
+        return e == cudaSuccess ? DRESSX_OK : DRESSX_ECUDA;
+    }
+    unsigned long long *A = (unsigned long long *)(base + NA_A);
+    unsigned long long *B = (unsigned long long *)(base + NA_B);
+    long long *offs = (long long *)(base + NA_OFFS);
+    int *counts = (int *)(base + NA_COUNTS);
+    Tile *tiles = (Tile *)(base + NA_TILESB);
+    long long *heads = (long long *)(base + NA_HEADS);
+    long long *tbase = (long long *)(base + NA_BASE);
+    long long *seg_begin = (long long *)(base + NA_SEG);
+    long long *seg_end = seg_begin + 1;
+    int *seg_tile0 = (int *)(seg_begin + 2);
+    int *moves = seg_tile0 + 2;
+    const int nt = (int)((n + TILE - 1) / TILE);
+
+    // every scratch word read below is written first in this call, so the
+    // array needs no clearing between calls
+    count_launch(), k_na_setup<<<1, 256, 0, st>>>(n, nt, tiles, seg_begin, seg_end, seg_tile0);
+    count_launch(), k_na_load<<<(unsigned)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024), 256, 0, st>>>(n, values, A);
+    unsigned long long *a = A, *b = B;
+    for (int pass = 0; pass < 8; ++pass) {           // even pass count: sorted keys end in A
+        const int shift = 8 * pass;
+        count_launch(), k_tile_hist<<<nt, HT, 0, st>>>(tiles, a, shift, counts);
+        count_launch(), k_seg_offsets<<<1, RADIX, 0, st>>>(seg_begin, seg_tile0, counts, offs, moves);
+        count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(tiles, a, b, shift, offs);
+        unsigned long long *t = a;
+        a = b;
+        b = t;
+    }
+    count_launch(), k_tile_heads<<<nt, HT, 0, st>>>(tiles, seg_begin, A, heads);
+    count_launch(), k_na_scan<<<1, 32, 0, st>>>(heads, nt, tbase);
+    long long *starts = (long long *)B;               // B is free once the keys are sorted into A
+    long long *out_pairs = (long long *)pairs;
+    count_launch(), k_na_runs<<<nt, HT, 0, st>>>(tiles, A, tbase, starts, out_pairs);
+    count_launch(), k_na_counts<<<(unsigned)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024), 256, 0, st>>>(
+        n, nt, tbase, starts, out_pairs, (long long *)num_runs);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::fprintf(stderr, "dress_b200: dressx_histogram_noalloc: launch: %s\n", cudaGetErrorString(e));
+        return DRESSX_ECUDA;
+    }
+    return DRESSX_OK;
+}

@@ -95,7 +95,11 @@ SIGNATURES = {
     "dressx_batch_destroy": (None, [ctypes.c_void_p]),
     "dressx_stream": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p)]),
     "dressx_counters": (ctypes.c_int, [_c_i64_p, _c_i64_p, _c_i64_p, ctypes.c_int]),
+    "dressx_histogram_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p]),
 }
+
+NOALLOC_MAX_VALUES = 1 << 20          # DRESSX_NOALLOC_MAX_VALUES
 
 _lib = None
 

@@ -123,6 +123,31 @@ int dressx_stream(void **stream);
  * device->host by this library, and kernels it launched. */
 int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, int reset);
 
+/* ---- Histogram without allocation -------------------------------------
+ * No counterpart in the reference.  Exact (value, count) histogram of n
+ * doubles that already sit in device memory, for callers that cannot
+ * allocate device memory when they need it: code running while a CUDA graph
+ * is captured, frameworks whose caching allocator owns the device memory,
+ * and loops that must not allocate after start-up.  The call allocates
+ * nothing: its scratch is one fixed array of about 16.5 MiB compiled into the
+ * library, which every GPU that loads the library holds until the process
+ * exits.
+ *   values   device pointer, n doubles (n <= DRESSX_NOALLOC_MAX_VALUES;
+ *            larger n returns DRESSX_EUNSUPPORTED and enqueues nothing)
+ *   pairs    device pointer, room for 2*n int64: [value bits, count, ...]
+ *            ascending by value, ==-equal values merged as in
+ *            dressx_hist_batch
+ *   num_runs device pointer, one int64: the number of (value, count) pairs
+ *   stream   cudaStream_t the work is enqueued on (NULL = legacy stream)
+ * Nothing is synchronised: results are valid once the stream has run the
+ * enqueued work.  The first call on a device looks up the array's device
+ * address; make that first call before any stream capture starts.  Every
+ * call uses the same array, so calls whose work overlaps on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller. */
+#define DRESSX_NOALLOC_MAX_VALUES (1 << 20)
+int dressx_histogram_noalloc(const double *values, int64_t n, int64_t *pairs, int64_t *num_runs,
+                             void *stream);
+
 /* Frees a buffer returned by this library. */
 void dressx_free(void *p);
 
