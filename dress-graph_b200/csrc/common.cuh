@@ -23,11 +23,15 @@ __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a,
 __device__ __forceinline__ double dsqrt(double a) { return __dsqrt_rn(a); }
 
 // One Neumaier step: s <- s + b with the lost low part accumulated in c.
+// The larger-magnitude operand is picked by a select rather than a branch:
+// the same two operations in the same order as the reference's if/else
+// (libdress/src/dress.c:58-62), with no branch in the serial chain.
 __device__ __forceinline__ void kbn_step(double &s, double &c, double b)
 {
     double t = dadd(s, b);
-    double e = (fabs(s) >= fabs(b)) ? dadd(dsub(s, t), b) : dadd(dsub(b, t), s);
-    c = dadd(c, e);
+    bool g = fabs(s) >= fabs(b);
+    double big = g ? s : b, small = g ? b : s;
+    c = dadd(c, dadd(dsub(big, t), small));
     s = t;
 }
 

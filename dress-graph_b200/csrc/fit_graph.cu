@@ -23,6 +23,7 @@
 // folds max|d_next - d| into a per-sweep slot, and every kernel of sweep i
 // returns at once if sweep i-1 already met the tolerance, so a chunk of
 // sweeps is launched back to back and the host reads the slots once per chunk.
+#include <algorithm>
 #include <climits>
 #include <chrono>
 #include <cstring>
@@ -30,21 +31,14 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "sweep.cuh"
 
 namespace dress {
 namespace {
 
-constexpr int NB = 8;
 constexpr int RING = 64;           // per-sweep convergence slots
 constexpr int MAX_CHUNK = 32;      // sweeps launched per host check (<= RING/2)
-constexpr int WARP_CAP = 1024;     // terms one warp sorts in shared memory
-enum { B1 = 0, B2, B4, B8, B16, B32, BWARP, BBLOCK };
-
-__host__ __device__ __forceinline__ int bin_of(long long n)
-{
-    return n <= 1 ? B1 : n <= 2 ? B2 : n <= 4 ? B4 : n <= 8 ? B8 : n <= 16 ? B16
-         : n <= 32 ? B32 : n <= WARP_CAP ? BWARP : BBLOCK;
-}
+using namespace sweep;
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
@@ -245,6 +239,16 @@ __global__ void k_bin_scatter(int n, const int *len, int add, int *cursor, int *
     }
 }
 
+__global__ void k_gather_seg(int n, const int *perm, const int *len, int *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = len[perm[i]];
+}
+
+__global__ void k_fix_inv(int n, int base, const int *perm, int *inv)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) inv[perm[base + i]] = base + i;
+}
+
 __global__ void k_gather_deg(int N, const int *vperm, const int *deg, int *ndeg)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
@@ -303,258 +307,6 @@ __global__ void k_unpermute(int n, const int *perm, const double *src, double *d
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         dst[perm[i]] = src[i];
-}
-
-// ------------------------------------------------------------------------
-// sweep kernels
-// ------------------------------------------------------------------------
-
-struct Sweep {
-    int N, E, fwd;                 // fwd: FORWARD/BACKWARD self term
-    const long long *row_off;      // [N+1] renumbered CSR rows
-    const int *row_eid;            // [S]
-    const int *eu, *ev;            // [E]
-    const double *w;               // [E] (weighted graphs)
-    double wc;                     // the weight when all are equal
-    const double *nw;              // [N]
-    const long long *ioff;         // [E+1]
-    const int2 *pairs;             // [T]
-    double *vd;                    // [N]
-    unsigned long long *maxd;      // [max_iterations]
-    const double *d, *p;           // current values and products
-    double *dn, *pn;               // next values and products
-    int iter, slot, prev_slot;     // sweep index and its convergence slots
-    double eps;
-    double *scratch;               // block-bin spill area (rows larger than shared memory)
-    long long scratch_stride;
-};
-
-template <bool UNIF>
-__device__ __forceinline__ double prod(const Sweep &s, int e)
-{
-    return UNIF ? dmul(s.wc, s.d[e]) : s.p[e];
-}
-
-template <bool UNIF>
-__device__ __forceinline__ double self_term(const Sweep &s, int j, int u, int v)
-{
-    double own = prod<UNIF>(s, j);
-    double a = dmul(4.0, s.nw[u]);
-    if (s.fwd) return dadd(a, own);
-    return dadd(dadd(a, dmul(4.0, s.nw[v])), dmul(2.0, own));
-}
-
-// edge value from its sorted-KBN numerator; also stores d_next (and p_next)
-template <bool UNIF>
-__device__ __forceinline__ double finish_edge(const Sweep &s, int j, int u, int v, double num)
-{
-    double den = dmul(s.vd[u], s.vd[v]);
-    double r = den > 0.0 ? ddiv(num, den) : 0.0;
-    s.dn[j] = r;
-    if (!UNIF) s.pn[j] = dmul(s.w[j], r);
-    return fabs(dsub(s.d[j], r));
-}
-
-// ---- one thread per item, M-term register network ----
-template <int M, bool UNIF>
-__global__ void __launch_bounds__(128) k_vertex_thr(Sweep s, int begin, int end)
-{
-    if (s.iter > 0 && __longlong_as_double((long long)s.maxd[s.prev_slot]) < s.eps) return;
-    int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= end) return;
-    long long b = s.row_off[i];
-    int deg = (int)(s.row_off[i + 1] - b);
-    double a[M];
-    a[0] = dmul(4.0, s.nw[i]);
-#pragma unroll
-    for (int k = 1; k < M; ++k) a[k] = (k <= deg) ? prod<UNIF>(s, s.row_eid[b + k - 1]) : DRESS_INF;
-    if (M > 1) sort_regs<M>(a);
-    s.vd[i] = dsqrt(kbn_regs<M>(a, deg + 1));
-}
-
-template <int M, bool UNIF>
-__global__ void __launch_bounds__(128) k_edge_thr(Sweep s, int begin, int end)
-{
-    if (s.iter > 0 && __longlong_as_double((long long)s.maxd[s.prev_slot]) < s.eps) return;
-    int j = begin + blockIdx.x * blockDim.x + threadIdx.x;
-    double delta = 0.0;
-    if (j < end) {
-        int u = s.eu[j], v = s.ev[j];
-        double self = self_term<UNIF>(s, j, u, v);
-        double num;
-        if (M == 1) {
-            num = dadd(self, 0.0);           // sorted KBN of a single term
-        } else {
-            long long o = s.ioff[j];
-            int nc = (int)(s.ioff[j + 1] - o);
-            double a[M];
-#pragma unroll
-            for (int k = 0; k < M; ++k) {
-                if (k < nc) {
-                    int2 pr = s.pairs[o + k];
-                    a[k] = dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
-                } else {
-                    a[k] = (k == nc) ? self : DRESS_INF;
-                }
-            }
-            sort_regs<M>(a);
-            num = kbn_regs<M>(a, nc + 1);
-        }
-        delta = finish_edge<UNIF>(s, j, u, v, num);
-    }
-    block_max_to(&s.maxd[s.slot], delta);
-}
-
-// ---- one warp per item, shared-memory sort ----
-struct WarpSync { __device__ void operator()() const { __syncwarp(); } };
-struct BlockSync { __device__ void operator()() const { __syncthreads(); } };
-
-template <bool UNIF>
-__global__ void __launch_bounds__(256) k_vertex_warp(Sweep s, int begin, int end)
-{
-    extern __shared__ double sm[];
-    if (s.iter > 0 && __longlong_as_double((long long)s.maxd[s.prev_slot]) < s.eps) return;
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    double *buf = sm + (size_t)wid * WARP_CAP;
-    for (int i = begin + blockIdx.x * nw + wid; i < end; i += gridDim.x * nw) {
-        long long b = s.row_off[i];
-        int deg = (int)(s.row_off[i + 1] - b), n = deg + 1;
-        if (lane == 0) buf[0] = dmul(4.0, s.nw[i]);
-        for (int k = lane; k < deg; k += 32) buf[k + 1] = prod<UNIF>(s, s.row_eid[b + k]);
-        __syncwarp();
-        sort_shared(buf, n, lane, 32, WarpSync());
-        if (lane == 0) s.vd[i] = dsqrt(kbn_sorted_buf(buf, n));
-        __syncwarp();
-    }
-}
-
-template <bool UNIF>
-__global__ void __launch_bounds__(256) k_edge_warp(Sweep s, int begin, int end)
-{
-    extern __shared__ double sm[];
-    if (s.iter > 0 && __longlong_as_double((long long)s.maxd[s.prev_slot]) < s.eps) return;
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    double *buf = sm + (size_t)wid * WARP_CAP;
-    double delta = 0.0;
-    for (int j = begin + blockIdx.x * nw + wid; j < end; j += gridDim.x * nw) {
-        int u = s.eu[j], v = s.ev[j];
-        long long o = s.ioff[j];
-        int nc = (int)(s.ioff[j + 1] - o);
-        for (int k = lane; k < nc; k += 32) {
-            int2 pr = s.pairs[o + k];
-            buf[k] = dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
-        }
-        if (lane == 0) buf[nc] = self_term<UNIF>(s, j, u, v);
-        __syncwarp();
-        sort_shared(buf, nc + 1, lane, 32, WarpSync());
-        if (lane == 0) delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_sorted_buf(buf, nc + 1)));
-        __syncwarp();
-    }
-    block_max_to(&s.maxd[s.slot], delta);
-}
-
-// ---- one block per item (hub rows / hub edges) ----
-template <bool UNIF>
-__global__ void __launch_bounds__(512) k_vertex_block(Sweep s, int begin, int end, int cap)
-{
-    extern __shared__ double sm[];
-    if (s.iter > 0 && __longlong_as_double((long long)s.maxd[s.prev_slot]) < s.eps) return;
-    for (int i = begin + blockIdx.x; i < end; i += gridDim.x) {
-        long long b = s.row_off[i];
-        int deg = (int)(s.row_off[i + 1] - b), n = deg + 1;
-        double *buf = n <= cap ? sm : s.scratch + (long long)blockIdx.x * s.scratch_stride;
-        if (threadIdx.x == 0) buf[0] = dmul(4.0, s.nw[i]);
-        for (int k = threadIdx.x; k < deg; k += blockDim.x) buf[k + 1] = prod<UNIF>(s, s.row_eid[b + k]);
-        __syncthreads();
-        sort_shared(buf, n, threadIdx.x, blockDim.x, BlockSync());
-        if (threadIdx.x == 0) s.vd[i] = dsqrt(kbn_sorted_buf(buf, n));
-        __syncthreads();
-    }
-}
-
-template <bool UNIF>
-__global__ void __launch_bounds__(512) k_edge_block(Sweep s, int begin, int end, int cap)
-{
-    extern __shared__ double sm[];
-    if (s.iter > 0 && __longlong_as_double((long long)s.maxd[s.prev_slot]) < s.eps) return;
-    double delta = 0.0;
-    for (int j = begin + blockIdx.x; j < end; j += gridDim.x) {
-        int u = s.eu[j], v = s.ev[j];
-        long long o = s.ioff[j];
-        int nc = (int)(s.ioff[j + 1] - o);
-        double *buf = nc + 1 <= cap ? sm : s.scratch + (long long)blockIdx.x * s.scratch_stride;
-        for (int k = threadIdx.x; k < nc; k += blockDim.x) {
-            int2 pr = s.pairs[o + k];
-            buf[k] = dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
-        }
-        if (threadIdx.x == 0) buf[nc] = self_term<UNIF>(s, j, u, v);
-        __syncthreads();
-        sort_shared(buf, nc + 1, threadIdx.x, blockDim.x, BlockSync());
-        if (threadIdx.x == 0) delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_sorted_buf(buf, nc + 1)));
-        __syncthreads();
-    }
-    block_max_to(&s.maxd[s.slot], delta);
-}
-
-// ------------------------------------------------------------------------
-// host side
-// ------------------------------------------------------------------------
-
-inline unsigned grid_for(long long n, int threads, int cap_blocks)
-{
-    long long b = (n + threads - 1) / threads;
-    if (b < 1) b = 1;
-    if (b > cap_blocks) b = cap_blocks;
-    return (unsigned)b;
-}
-
-struct Bins {
-    int start[NB + 1];
-    long long max_terms_block;   // largest item in the block bin
-};
-
-template <bool UNIF>
-Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, int sms, int block_cap,
-                    cudaStream_t st)
-{
-    const int T = 128;
-    // hub items first: they carry the longest sequential sums
-    if (vb.start[BBLOCK + 1] > vb.start[BBLOCK]) {
-        int n = vb.start[BBLOCK + 1] - vb.start[BBLOCK];
-        count_launch(), k_vertex_block<UNIF><<<grid_for(n, 1, 2 * sms), 512, (size_t)block_cap * 8, st>>>(
-            s, vb.start[BBLOCK], vb.start[BBLOCK + 1], block_cap);
-    }
-    if (vb.start[BWARP + 1] > vb.start[BWARP]) {
-        int n = vb.start[BWARP + 1] - vb.start[BWARP];
-        count_launch(), k_vertex_warp<UNIF><<<grid_for(n, 8, 8 * sms), 256, 8 * WARP_CAP * 8, st>>>(
-            s, vb.start[BWARP], vb.start[BWARP + 1]);
-    }
-#define DRESS_VTHR(BIN, M)                                                                   \
-    if (vb.start[BIN + 1] > vb.start[BIN])                                                   \
-        count_launch(), k_vertex_thr<M, UNIF><<<grid_for(vb.start[BIN + 1] - vb.start[BIN], T, INT_MAX), T, 0, st>>>( \
-            s, vb.start[BIN], vb.start[BIN + 1]);
-    DRESS_VTHR(B32, 32) DRESS_VTHR(B16, 16) DRESS_VTHR(B8, 8) DRESS_VTHR(B4, 4) DRESS_VTHR(B2, 2)
-    DRESS_VTHR(B1, 1)
-#undef DRESS_VTHR
-    if (eb.start[BBLOCK + 1] > eb.start[BBLOCK]) {
-        int n = eb.start[BBLOCK + 1] - eb.start[BBLOCK];
-        count_launch(), k_edge_block<UNIF><<<grid_for(n, 1, 2 * sms), 512, (size_t)block_cap * 8, st>>>(
-            s, eb.start[BBLOCK], eb.start[BBLOCK + 1], block_cap);
-    }
-    if (eb.start[BWARP + 1] > eb.start[BWARP]) {
-        int n = eb.start[BWARP + 1] - eb.start[BWARP];
-        count_launch(), k_edge_warp<UNIF><<<grid_for(n, 8, 8 * sms), 256, 8 * WARP_CAP * 8, st>>>(
-            s, eb.start[BWARP], eb.start[BWARP + 1]);
-    }
-#define DRESS_ETHR(BIN, M)                                                                   \
-    if (eb.start[BIN + 1] > eb.start[BIN])                                                   \
-        count_launch(), k_edge_thr<M, UNIF><<<grid_for(eb.start[BIN + 1] - eb.start[BIN], T, INT_MAX), T, 0, st>>>( \
-            s, eb.start[BIN], eb.start[BIN + 1]);
-    DRESS_ETHR(B32, 32) DRESS_ETHR(B16, 16) DRESS_ETHR(B8, 8) DRESS_ETHR(B4, 4) DRESS_ETHR(B2, 2)
-    DRESS_ETHR(B1, 1)
-#undef DRESS_ETHR
-    DRESS_CUDA_TRY(cudaGetLastError());
-    return Status::Ok();
 }
 
 template <class T>
@@ -706,8 +458,8 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_einv.alloc((size_t)E, st));
     DRESS_CUDA_TRY(cudaMemsetAsync(d_bc.get(), 0, 4 * NB * sizeof(int), st));
     const int vg = (int)grid_for(N, 256, 32 * sms);
-    count_launch(), k_bin_count<<<vg, 256, 0, st>>>(N, d_deg.get(), 1, d_bc.get());
-    count_launch(), k_bin_count<<<eg, 256, 0, st>>>(E, d_cnt.get(), 1, d_bc.get() + NB);
+    count_launch(), k_bin_count<<<vg, 256, 0, st>>>(N, d_deg.get(), 0, d_bc.get());
+    count_launch(), k_bin_count<<<eg, 256, 0, st>>>(E, d_cnt.get(), 0, d_bc.get() + NB);
     int bc[2 * NB];
     DRESS_CUDA_TRY(counted_memcpy(bc, d_bc.get(), sizeof(bc), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
@@ -722,8 +474,60 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     int cur[2 * NB];
     for (int b = 0; b < NB; ++b) { cur[b] = vb.start[b]; cur[NB + b] = eb.start[b]; }
     DRESS_CUDA_TRY(counted_memcpy(d_bc.get() + 2 * NB, cur, sizeof(cur), cudaMemcpyHostToDevice, st));
-    count_launch(), k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), 1, d_bc.get() + 2 * NB, d_vperm.get(), d_vinv.get());
-    count_launch(), k_bin_scatter<<<eg, 256, 0, st>>>(E, d_cnt.get(), 1, d_bc.get() + 3 * NB, d_eperm.get(), d_einv.get());
+    count_launch(), k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), 0, d_bc.get() + 2 * NB, d_vperm.get(), d_vinv.get());
+    count_launch(), k_bin_scatter<<<eg, 256, 0, st>>>(E, d_cnt.get(), 0, d_bc.get() + 3 * NB, d_eperm.get(), d_einv.get());
+    // block items largest first, so the longest sequential sums start first
+    {
+        struct Seg { int *perm, *inv; const int *len; int b0, b1; };
+        Seg segs[4] = {{d_vperm.get(), d_vinv.get(), d_deg.get(), vb.start[BBLOCK], vb.start[BBLOCK + 1]},
+                       {d_vperm.get(), d_vinv.get(), d_deg.get(), vb.start[BBIG], vb.start[BBIG + 1]},
+                       {d_eperm.get(), d_einv.get(), d_cnt.get(), eb.start[BBLOCK], eb.start[BBLOCK + 1]},
+                       {d_eperm.get(), d_einv.get(), d_cnt.get(), eb.start[BBIG], eb.start[BBIG + 1]}};
+        for (const Seg &g2 : segs) {
+            const int n = g2.b1 - g2.b0;
+            if (n < 2) continue;
+            DevBuf<int> d_len;
+            DRESS_TRY(d_len.alloc((size_t)n, st));
+            count_launch(), k_gather_seg<<<grid_for(n, 256, 64 * sms), 256, 0, st>>>(n, g2.perm + g2.b0, g2.len, d_len.get());
+            std::vector<int> perm((size_t)n), len((size_t)n), idx((size_t)n);
+            DRESS_CUDA_TRY(counted_memcpy(perm.data(), g2.perm + g2.b0, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
+            DRESS_CUDA_TRY(counted_memcpy(len.data(), d_len.get(), (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
+            DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+            for (int i = 0; i < n; ++i) idx[(size_t)i] = i;
+            std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return len[(size_t)a] > len[(size_t)b]; });
+            std::vector<int> sorted((size_t)n);
+            for (int i = 0; i < n; ++i) sorted[(size_t)i] = perm[(size_t)idx[(size_t)i]];
+            DRESS_CUDA_TRY(counted_memcpy(g2.perm + g2.b0, sorted.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st));
+            count_launch(), k_fix_inv<<<grid_for(n, 256, 64 * sms), 256, 0, st>>>(n, g2.b0, g2.perm, g2.inv);
+            DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+    }
+
+    // per-item slots for the sorted terms of the block items (both block bins)
+    DevBuf<long long> d_bofs_v, d_bofs_e;
+    DevBuf<double> d_bkey_v, d_bkey_e;
+    {
+        struct Blk { int *perm; const int *len; int b0, b1; DevBuf<long long> *ofs; DevBuf<double> *keys; };
+        Blk blks[2] = {{d_vperm.get(), d_deg.get(), vb.start[BBLOCK], vb.start[BBIG + 1], &d_bofs_v, &d_bkey_v},
+                       {d_eperm.get(), d_cnt.get(), eb.start[BBLOCK], eb.start[BBIG + 1], &d_bofs_e, &d_bkey_e}};
+        for (Blk &k : blks) {
+            const int n = k.b1 - k.b0;
+            DRESS_TRY(k.ofs->alloc((size_t)n + 1, st));
+            std::vector<long long> ofs((size_t)n + 1, 0);
+            if (n > 0) {
+                DevBuf<int> d_len;
+                DRESS_TRY(d_len.alloc((size_t)n, st));
+                count_launch(), k_gather_seg<<<grid_for(n, 256, 64 * sms), 256, 0, st>>>(n, k.perm + k.b0, k.len, d_len.get());
+                std::vector<int> len((size_t)n);
+                DRESS_CUDA_TRY(counted_memcpy(len.data(), d_len.get(), (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
+                DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+                for (int i = 0; i < n; ++i) ofs[(size_t)i + 1] = ofs[(size_t)i] + len[(size_t)i];
+            }
+            DRESS_CUDA_TRY(counted_memcpy(k.ofs->get(), ofs.data(), ((size_t)n + 1) * sizeof(long long),
+                                          cudaMemcpyHostToDevice, st));
+            DRESS_TRY(k.keys->alloc((size_t)(ofs[(size_t)n] > 0 ? ofs[(size_t)n] : 1), st));
+        }
+    }
 
     DevBuf<int> d_ndeg, d_row_eid, d_eu, d_ev, d_ncnt;
     DevBuf<long long> d_row_off, d_ioff;
@@ -765,25 +569,22 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     // block-bin shared memory and spill area
     int smem_optin = 0;
     DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, en.device));
-    int block_cap = (smem_optin - 1024) / 8;
-    // largest block-bin item (rows have max_row + 1 terms, edges at most that)
+    // keys (8 B) and payload (8 B edge pair, 4 B row slot) per stored term,
+    // leaving room for static shared memory
+    int block_cap = (smem_optin - 1024) / 16;
+    int vblock_cap = (smem_optin - 1024) / 12;
+    // largest block-bin item: a row has at most max_row stored terms, an edge fewer
     long long big = 0;
-    if (vb.start[BBLOCK + 1] > vb.start[BBLOCK] || eb.start[BBLOCK + 1] > eb.start[BBLOCK])
-        big = max_row + 1;
-    DevBuf<double> d_scratch;
+    if ((vb.has(BBIG) && max_row > vblock_cap) || (eb.has(BBIG) && max_row > block_cap)) big = max_row;
+    DevBuf<double> d_scratch_k;
+    DevBuf<int2> d_scratch_v;
     long long scratch_stride = 0;
     if (big > block_cap) {
         scratch_stride = big;
-        DRESS_TRY(d_scratch.alloc((size_t)(2 * sms) * (size_t)big, st));
+        DRESS_TRY(d_scratch_v.alloc((size_t)(2 * sms) * (size_t)big, st));
     }
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_block<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, block_cap * 8));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_block<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, block_cap * 8));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_block<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, block_cap * 8));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_block<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, block_cap * 8));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * WARP_CAP * 8));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * WARP_CAP * 8));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * WARP_CAP * 8));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_warp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * WARP_CAP * 8));
+    DRESS_TRY(set_sweep_attributes<true>(block_cap, vblock_cap));
+    DRESS_TRY(set_sweep_attributes<false>(block_cap, vblock_cap));
 
     DevBuf<unsigned long long> d_maxd;
     DRESS_TRY(d_vd.alloc((size_t)(N > 0 ? N : 1), st));
@@ -806,7 +607,17 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     s.ioff = d_ioff.get(); s.pairs = d_pairs.get();
     s.vd = d_vd.get(); s.maxd = d_maxd.get();
     s.eps = epsilon;
-    s.scratch = d_scratch.get(); s.scratch_stride = scratch_stride;
+    s.scratch_k = d_scratch_k.get(); s.scratch_v = d_scratch_v.get(); s.scratch_stride = scratch_stride;
+    DevBuf<int> d_qv, d_qe;
+    DevBuf<unsigned> d_qcount;
+    DRESS_TRY(d_qv.alloc((size_t)(N > 0 ? N : 1), st));
+    DRESS_TRY(d_qe.alloc((size_t)(E > 0 ? E : 1), st));
+    DRESS_TRY(d_qcount.alloc(2, st));
+    s.qv = d_qv.get(); s.qe = d_qe.get(); s.qcount = d_qcount.get();
+    s.bkey_v = d_bkey_v.get(); s.bkey_e = d_bkey_e.get();
+    s.bofs_v = d_bofs_v.get(); s.bofs_e = d_bofs_e.get();
+    s.bv0 = vb.start[BBLOCK]; s.be0 = eb.start[BBLOCK];
+    LaunchCfg lc{sms, block_cap, vblock_cap, st, en.side, en.fork, en.join};
     double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + E};
     double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + E};
 
@@ -826,8 +637,8 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
             s.prev_slot = (it + RING - 1) % RING;
             s.d = dbuf[it & 1]; s.dn = dbuf[(it + 1) & 1];
             s.p = pbuf[it & 1]; s.pn = pbuf[(it + 1) & 1];
-            if (uniform) DRESS_TRY(launch_sweep<true>(s, vb, eb, sms, block_cap, st));
-            else         DRESS_TRY(launch_sweep<false>(s, vb, eb, sms, block_cap, st));
+            if (uniform) DRESS_TRY(launch_sweep<true>(s, vb, eb, lc));
+            else         DRESS_TRY(launch_sweep<false>(s, vb, eb, lc));
         }
         DRESS_CUDA_TRY(counted_memcpy(hmax, d_maxd.get(), RING * sizeof(unsigned long long),
                                        cudaMemcpyDeviceToHost, st));

@@ -1,0 +1,749 @@
+// sweep.cuh -- the per-sweep kernels of the single-graph fit (fit_graph.cu).
+//
+// Reference: libdress/src/dress.c:556-591 (vertex norms, edge update) with
+// the sorted KBN sum of dress.c:51-66.
+//
+// Items (vertices, edges) are binned by their number of STORED terms: the
+// row's slots for a vertex, the common-neighbour pairs for an edge.  Every
+// item has one more term, its self term (4*nw for a vertex, the self/own-edge
+// term for an edge), which is merged into the sorted sequence at its rank.
+//
+// Persistent order: the storage order of a row's slots (row_eid) and of an
+// edge's pairs is irrelevant to the result (the sum sorts its terms), so each
+// sweep keeps them in the order of the previous sweep's values.  A sweep
+// gathers the terms in stored order, checks that they are ascending, and only
+// when they are not sorts them (carrying the slot / pair along) and writes the
+// new order back.  Once the values settle, most items skip the sort.
+//
+//   bins: 0 stored terms; <=2, <=4, <=8, <=16 (one thread per item, register
+//   network); <=MED_CAP (one thread per item streaming its terms: the sum runs
+//   while the order is checked; an item found out of order is queued, sorted
+//   by a warp and streamed again); more (one block per item, shared memory,
+//   largest items first; rows beyond the shared capacity spill to a global
+//   slab).  The block items are split at BIG_CAP so that the smaller ones run
+//   several blocks per SM.
+#pragma once
+#include <climits>
+
+#include "common.cuh"
+#include "engine.h"
+
+namespace dress {
+namespace sweep {
+
+constexpr int NB = 8;
+constexpr int MED_CAP = 512;        // stored terms of a streamed (one-thread) item
+constexpr int BIG_CAP = 4096;       // block items up to this share an SM
+enum { B0 = 0, B2, B4, B8, B16, BMED, BBLOCK, BBIG };
+
+__host__ __device__ __forceinline__ int bin_of(long long n)
+{
+    return n == 0 ? B0 : n <= 2 ? B2 : n <= 4 ? B4 : n <= 8 ? B8 : n <= 16 ? B16 : n <= MED_CAP ? BMED
+         : n <= BIG_CAP ? BBLOCK : BBIG;
+}
+
+struct Sweep {
+    int N, E, fwd;                 // fwd: FORWARD/BACKWARD self term
+    const long long *row_off;      // [N+1] renumbered CSR rows
+    int *row_eid;                  // [S]  slot edge ids, kept in value order
+    const int *eu, *ev;            // [E]
+    const double *w;               // [E] (weighted graphs)
+    double wc;                     // the weight when all are equal
+    const double *nw;              // [N]
+    const long long *ioff;         // [E+1]
+    int2 *pairs;                   // [T]  common-neighbour edge pairs, kept in value order
+    double *vd;                    // [N]
+    unsigned long long *maxd;      // convergence ring
+    const double *d, *p;           // current values and products
+    double *dn, *pn;               // next values and products
+    int iter, slot, prev_slot;     // sweep index and its convergence slots
+    double eps;
+    double *scratch_k;             // block-bin spill (keys), per block
+    int2 *scratch_v;               // block-bin spill (payload), per block
+    long long scratch_stride;
+    int *qv, *qe;                  // streamed items found out of order (vertices, edges)
+    unsigned *qcount;              // [2] queue lengths
+    double *bkey_v, *bkey_e;       // sorted terms of the block items, one slot per item
+    const long long *bofs_v, *bofs_e;   // slot offsets, indexed from bv0 / be0
+    int bv0, be0;                  // first block item (vertex, edge)
+};
+
+__device__ __forceinline__ bool skipped(const Sweep &s)
+{
+    return s.iter > 0 && __longlong_as_double((long long)s.maxd[s.prev_slot]) < s.eps;
+}
+
+template <bool UNIF>
+__device__ __forceinline__ double prod(const Sweep &s, int e)
+{
+    return UNIF ? dmul(s.wc, s.d[e]) : s.p[e];
+}
+
+template <bool UNIF>
+__device__ __forceinline__ double self_term(const Sweep &s, int j, int u, int v)
+{
+    double own = prod<UNIF>(s, j);
+    double a = dmul(4.0, s.nw[u]);
+    if (s.fwd) return dadd(a, own);
+    return dadd(dadd(a, dmul(4.0, s.nw[v])), dmul(2.0, own));
+}
+
+// edge value from its numerator; stores d_next (and p_next), returns |delta|
+template <bool UNIF>
+__device__ __forceinline__ double finish_edge(const Sweep &s, int j, int u, int v, double num)
+{
+    double den = dmul(s.vd[u], s.vd[v]);
+    double r = den > 0.0 ? ddiv(num, den) : 0.0;
+    s.dn[j] = r;
+    if (!UNIF) s.pn[j] = dmul(s.w[j], r);
+    return fabs(dsub(s.d[j], r));
+}
+
+// ---- register helpers -------------------------------------------------------------
+
+template <class P>
+__device__ __forceinline__ void cswap_kv(double &a, double &b, P &x, P &y)
+{
+    bool sw = b < a;
+    double lo = sw ? b : a, hi = sw ? a : b;
+    P plo = sw ? y : x, phi = sw ? x : y;
+    a = lo; b = hi; x = plo; y = phi;
+}
+
+// single-direction bitonic network on M registers, payload carried along
+template <int M, class P>
+__device__ __forceinline__ void sort_kv(double (&a)[M], P (&v)[M])
+{
+#pragma unroll
+    for (int k = 2; k <= M; k <<= 1) {
+#pragma unroll
+        for (int i = 0; i < M; ++i) {
+            int j = i ^ (k - 1);
+            if (j > i) cswap_kv(a[i], a[j], v[i], v[j]);
+        }
+#pragma unroll
+        for (int st = k >> 2; st > 0; st >>= 1) {
+#pragma unroll
+            for (int i = 0; i < M; ++i) {
+                int j = i ^ st;
+                if (j > i) cswap_kv(a[i], a[j], v[i], v[j]);
+            }
+        }
+    }
+}
+
+// Sorted KBN of a[0..n) (ascending, n <= M) with x merged in at its rank.
+template <int M>
+__device__ __forceinline__ double kbn_merge_regs(const double (&a)[M], int n, double x)
+{
+    int pos = 0;
+#pragma unroll
+    for (int k = 0; k < M; ++k) pos += (k < n && a[k] < x);
+    double s = pos == 0 ? x : a[0], c = 0.0;
+#pragma unroll
+    for (int t = 1; t <= M; ++t) {
+        if (t <= n) {
+            double v = t < pos ? a[t < M ? t : M - 1] : (t == pos ? x : a[t - 1]);
+            kbn_step(s, c, v);
+        }
+    }
+    return dadd(s, c);
+}
+
+// Sorted KBN of an ascending stream with one extra term x merged at its
+// rank (x goes before the first term >= x, exactly where kbn_merge_buf puts it).
+struct KbnStream {
+    double s, c, x;
+    bool started, inserted;
+    __device__ __forceinline__ explicit KbnStream(double extra) : s(0.0), c(0.0), x(extra), started(false), inserted(false) {}
+    __device__ __forceinline__ void raw(double v)
+    {
+        if (started) kbn_step(s, c, v);
+        else { s = v; started = true; }
+    }
+    __device__ __forceinline__ void push(double v)
+    {
+        if (!inserted && !(v < x)) { raw(x); inserted = true; }
+        raw(v);
+    }
+    __device__ __forceinline__ double finish()
+    {
+        if (!inserted) raw(x);
+        return dadd(s, c);
+    }
+};
+
+// Same over an ascending buffer (one thread).
+__device__ __forceinline__ double kbn_merge_buf(const double *a, int n, double x)
+{
+    int lo = 0, hi = n;                      // first index with a[idx] >= x
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    const int pos = lo;
+    double s, c = 0.0;
+    int i;
+    if (pos == 0) {
+        s = x;
+        i = 0;
+    } else {
+        s = a[0];
+        for (i = 1; i < pos; ++i) kbn_step(s, c, a[i]);
+        kbn_step(s, c, x);
+    }
+    // 8-term windows, the next window loaded while the current one is summed
+    if (i + 8 <= n) {
+        double cur[8], nxt[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) cur[t] = a[i + t];
+        while (i + 16 <= n) {
+#pragma unroll
+            for (int t = 0; t < 8; ++t) nxt[t] = a[i + 8 + t];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) kbn_step(s, c, cur[t]);
+#pragma unroll
+            for (int t = 0; t < 8; ++t) cur[t] = nxt[t];
+            i += 8;
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) kbn_step(s, c, cur[t]);
+        i += 8;
+    }
+    for (; i < n; ++i) kbn_step(s, c, a[i]);
+    return dadd(s, c);
+}
+
+// Cooperative ascending sort of keys[0..n) with payload (warp or block).
+template <class P, class Sync>
+__device__ __forceinline__ void sort_shared_kv(double *keys, P *vals, int n, int tid, int nthr, Sync sync)
+{
+    int M = 1;
+    while (M < n) M <<= 1;
+    for (int k = 2; k <= M; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int half = M >> 1;
+            for (int q = tid; q < half; q += nthr) {
+                int i = ((q & ~(j - 1)) << 1) | (q & (j - 1));
+                int p = (j == (k >> 1)) ? (i ^ (k - 1)) : (i | j);
+                int lo = i < p ? i : p, hi = i < p ? p : i;
+                if (hi < n) {
+                    double x = keys[lo], y = keys[hi];
+                    if (y < x) {
+                        keys[lo] = y;
+                        keys[hi] = x;
+                        P t = vals[lo];
+                        vals[lo] = vals[hi];
+                        vals[hi] = t;
+                    }
+                }
+            }
+            sync();
+        }
+    }
+}
+
+struct WarpSync { __device__ void operator()() const { __syncwarp(); } };
+struct BlockSync { __device__ void operator()() const { __syncthreads(); } };
+struct WarpAny { __device__ bool operator()(bool p) const { return __any_sync(0xffffffffu, p); } };
+struct BlockAny { __device__ bool operator()(bool p) const { return __syncthreads_or(p) != 0; } };
+
+// Restores ascending order of a nearly sorted keys[0..n) (payload carried):
+// odd-even transposition passes until one pass swaps nothing -- as many passes
+// as the farthest displacement -- and a full bitonic sort if that takes more
+// than MAX_PASSES passes.  Ends with all cooperating threads synchronised.
+constexpr int MAX_PASSES = 16;
+
+// fraction of descents above which the odd-even passes are skipped
+__device__ __forceinline__ bool far_from_sorted(int descents, int n) { return 8 * descents > n; }
+template <class P, class Sync, class Any>
+__device__ __forceinline__ void fix_order(double *keys, P *vals, int n, int tid, int nthr, Sync sync, Any any,
+                                          bool far = false)
+{
+    for (int pass = 0; pass < MAX_PASSES && !far; ++pass) {
+        bool sw = false;
+        for (int parity = 0; parity < 2; ++parity) {
+            for (int i = 2 * tid + parity; i + 1 < n; i += 2 * nthr) {
+                double x = keys[i], y = keys[i + 1];
+                if (y < x) {
+                    keys[i] = y;
+                    keys[i + 1] = x;
+                    P t = vals[i];
+                    vals[i] = vals[i + 1];
+                    vals[i + 1] = t;
+                    sw = true;
+                }
+            }
+            sync();
+        }
+        if (!any(sw)) return;
+    }
+    sort_shared_kv(keys, vals, n, tid, nthr, sync);
+}
+
+// ---- one thread per item (at most 16 stored terms) ----------------------------------
+
+template <int M, bool UNIF>
+__global__ void __launch_bounds__(128) k_vertex_thr(Sweep s, int begin, int end)
+{
+    if (skipped(s)) return;
+    const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end) return;
+    const double self = dmul(4.0, s.nw[i]);
+    if constexpr (M == 0) {
+        s.vd[i] = dsqrt(dadd(self, 0.0));
+    } else {
+        const long long b = s.row_off[i];
+        const int deg = (int)(s.row_off[i + 1] - b);
+        double a[M];
+        int id[M];
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            if (k < deg) {
+                id[k] = s.row_eid[b + k];
+                a[k] = prod<UNIF>(s, id[k]);
+            } else {
+                id[k] = -1;
+                a[k] = DRESS_INF;
+            }
+        }
+        bool sorted = true;
+#pragma unroll
+        for (int k = 0; k + 1 < M; ++k) sorted &= !(a[k + 1] < a[k]);
+        if (!sorted) {
+            sort_kv<M>(a, id);
+#pragma unroll
+            for (int k = 0; k < M; ++k)
+                if (k < deg) s.row_eid[b + k] = id[k];
+        }
+        s.vd[i] = dsqrt(kbn_merge_regs<M>(a, deg, self));
+    }
+}
+
+template <int M, bool UNIF>
+__global__ void __launch_bounds__(128) k_edge_thr(Sweep s, int begin, int end)
+{
+    if (skipped(s)) return;
+    const int j = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    double delta = 0.0;
+    if (j < end) {
+        const int u = s.eu[j], v = s.ev[j];
+        const double self = self_term<UNIF>(s, j, u, v);
+        double num;
+        if constexpr (M == 0) {
+            num = dadd(self, 0.0);               // sorted KBN of the single self term
+        } else {
+            const long long o = s.ioff[j];
+            const int nc = (int)(s.ioff[j + 1] - o);
+            double a[M];
+            int2 id[M];
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                if (k < nc) {
+                    id[k] = s.pairs[o + k];
+                    a[k] = dadd(prod<UNIF>(s, id[k].x), prod<UNIF>(s, id[k].y));
+                } else {
+                    id[k] = make_int2(-1, -1);
+                    a[k] = DRESS_INF;
+                }
+            }
+            bool sorted = true;
+#pragma unroll
+            for (int k = 0; k + 1 < M; ++k) sorted &= !(a[k + 1] < a[k]);
+            if (!sorted) {
+                sort_kv<M>(a, id);
+#pragma unroll
+                for (int k = 0; k < M; ++k)
+                    if (k < nc) s.pairs[o + k] = id[k];
+            }
+            num = kbn_merge_regs<M>(a, nc, self);
+        }
+        delta = finish_edge<UNIF>(s, j, u, v, num);
+    }
+    block_max_to(&s.maxd[s.slot], delta);
+}
+
+// ---- one thread per item, streamed (at most MED_CAP stored terms) ---------------------
+// The terms are gathered STREAM_D at a time (independent loads in flight),
+// summed in stored order while the order is checked; an item met out of
+// order is queued for k_*_med_sort, which sorts it and finishes it.
+constexpr int STREAM_D = 8;
+
+template <bool UNIF>
+__global__ void __launch_bounds__(256) k_vertex_med(Sweep s, int begin, int end)
+{
+    if (skipped(s)) return;
+    for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+        const long long b = s.row_off[i];
+        const int deg = (int)(s.row_off[i + 1] - b);
+        KbnStream ks(dmul(4.0, s.nw[i]));
+        double prev = -DRESS_INF;
+        bool ok = true;
+        for (int k = 0; k < deg && ok; k += STREAM_D) {
+            double v[STREAM_D];
+#pragma unroll
+            for (int t = 0; t < STREAM_D; ++t)
+                if (k + t < deg) v[t] = prod<UNIF>(s, s.row_eid[b + k + t]);
+#pragma unroll
+            for (int t = 0; t < STREAM_D; ++t) {
+                if (k + t < deg && ok) {
+                    if (v[t] < prev) ok = false;
+                    else { prev = v[t]; ks.push(v[t]); }
+                }
+            }
+        }
+        if (ok) s.vd[i] = dsqrt(ks.finish());
+        else s.qv[atomicAdd(&s.qcount[0], 1u)] = i;
+    }
+}
+
+template <bool UNIF>
+__global__ void __launch_bounds__(256) k_edge_med(Sweep s, int begin, int end)
+{
+    if (skipped(s)) return;
+    double delta = 0.0;
+    for (int j = begin + blockIdx.x * blockDim.x + threadIdx.x; j < end; j += gridDim.x * blockDim.x) {
+        const int u = s.eu[j], v = s.ev[j];
+        const long long o = s.ioff[j];
+        const int nc = (int)(s.ioff[j + 1] - o);
+        KbnStream ks(self_term<UNIF>(s, j, u, v));
+        double prev = -DRESS_INF;
+        bool ok = true;
+        for (int k = 0; k < nc && ok; k += STREAM_D) {
+            double x[STREAM_D];
+#pragma unroll
+            for (int t = 0; t < STREAM_D; ++t)
+                if (k + t < nc) {
+                    const int2 pr = s.pairs[o + k + t];
+                    x[t] = dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
+                }
+#pragma unroll
+            for (int t = 0; t < STREAM_D; ++t) {
+                if (k + t < nc && ok) {
+                    if (x[t] < prev) ok = false;
+                    else { prev = x[t]; ks.push(x[t]); }
+                }
+            }
+        }
+        if (ok) delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, ks.finish()));
+        else s.qe[atomicAdd(&s.qcount[1], 1u)] = j;
+    }
+    block_max_to(&s.maxd[s.slot], delta);
+}
+
+// one warp per queued item: restore ascending order, write it back, and sum
+// the sorted terms (lane 0) -- queued items are the minority
+template <bool UNIF>
+__global__ void __launch_bounds__(256) k_vertex_med_sort(Sweep s)
+{
+    extern __shared__ __align__(16) unsigned char smw[];
+    if (skipped(s)) return;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    double *kb = (double *)smw + (size_t)wid * MED_CAP;
+    int *pb = (int *)((double *)smw + (size_t)nwarps * MED_CAP) + (size_t)wid * MED_CAP;
+    const int n_items = (int)s.qcount[0];
+    for (int q = blockIdx.x * nwarps + wid; q < n_items; q += gridDim.x * nwarps) {
+        const int i = s.qv[q];
+        const long long b = s.row_off[i];
+        const int deg = (int)(s.row_off[i + 1] - b);
+        for (int k = lane; k < deg; k += 32) {
+            int e = s.row_eid[b + k];
+            pb[k] = e;
+            kb[k] = prod<UNIF>(s, e);
+        }
+        __syncwarp();
+        int d = 0;
+        for (int k = lane; k + 1 < deg; k += 32) d += kb[k + 1] < kb[k];
+        for (int o2 = 16; o2 > 0; o2 >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o2);
+        fix_order(kb, pb, deg, lane, 32, WarpSync(), WarpAny(), far_from_sorted(d, deg));
+        for (int k = lane; k < deg; k += 32) s.row_eid[b + k] = pb[k];
+        if (lane == 0) s.vd[i] = dsqrt(kbn_merge_buf(kb, deg, dmul(4.0, s.nw[i])));
+        __syncwarp();
+    }
+}
+
+template <bool UNIF>
+__global__ void __launch_bounds__(256) k_edge_med_sort(Sweep s)
+{
+    extern __shared__ __align__(16) unsigned char smw[];
+    if (skipped(s)) return;
+    double delta = 0.0;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    double *kb = (double *)smw + (size_t)wid * MED_CAP;
+    int2 *pb = (int2 *)((double *)smw + (size_t)nwarps * MED_CAP) + (size_t)wid * MED_CAP;
+    const int n_items = (int)s.qcount[1];
+    for (int q = blockIdx.x * nwarps + wid; q < n_items; q += gridDim.x * nwarps) {
+        const int j = s.qe[q];
+        const long long o = s.ioff[j];
+        const int nc = (int)(s.ioff[j + 1] - o);
+        for (int k = lane; k < nc; k += 32) {
+            int2 pr = s.pairs[o + k];
+            pb[k] = pr;
+            kb[k] = dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
+        }
+        __syncwarp();
+        int d = 0;
+        for (int k = lane; k + 1 < nc; k += 32) d += kb[k + 1] < kb[k];
+        for (int o2 = 16; o2 > 0; o2 >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o2);
+        fix_order(kb, pb, nc, lane, 32, WarpSync(), WarpAny(), far_from_sorted(d, nc));
+        for (int k = lane; k < nc; k += 32) s.pairs[o + k] = pb[k];
+        if (lane == 0) {
+            const int u = s.eu[j], v = s.ev[j];
+            delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_merge_buf(kb, nc, self_term<UNIF>(s, j, u, v))));
+        }
+        __syncwarp();
+    }
+    block_max_to(&s.maxd[s.slot], delta);
+}
+
+// ---- one block per item (hub rows, hub edges) -----------------------------------------
+// The block gathers the item's terms in stored order, restores ascending
+// order when needed (writing the new order back), and stores the sorted terms
+// in the item's slot of bkey_*; the sequential sums run afterwards, one thread
+// per item (k_*_block_sum), so no block idles behind a single summing thread.
+// Items beyond the shared capacity are sorted in place in their slot.
+
+template <bool UNIF, bool SUM_HERE>
+__global__ void __launch_bounds__(512) k_vertex_block(Sweep s, int begin, int end, int cap)   // cap: 12 B per term
+{
+    extern __shared__ __align__(16) unsigned char smb[];
+    __shared__ int descents;
+    if (skipped(s)) return;
+    for (int i = begin + blockIdx.x; i < end; i += gridDim.x) {
+        const long long b = s.row_off[i];
+        const int deg = (int)(s.row_off[i + 1] - b);
+        double *slot = s.bkey_v + s.bofs_v[i - s.bv0];
+        const bool inshm = deg <= cap;
+        double *kb = inshm ? (double *)smb : slot;
+        int *pb = inshm ? (int *)((double *)smb + cap) : (int *)(s.scratch_v + (long long)blockIdx.x * s.scratch_stride);
+        if (threadIdx.x == 0) descents = 0;
+        for (int k = threadIdx.x; k < deg; k += blockDim.x) {
+            int e = s.row_eid[b + k];
+            pb[k] = e;
+            kb[k] = prod<UNIF>(s, e);
+        }
+        __syncthreads();
+        int d = 0;
+        for (int k = threadIdx.x; k + 1 < deg; k += blockDim.x) d += kb[k + 1] < kb[k];
+        if (d) atomicAdd(&descents, d);
+        __syncthreads();
+        const int nd = descents;
+        if (nd) {
+            fix_order(kb, pb, deg, threadIdx.x, blockDim.x, BlockSync(), BlockAny(), far_from_sorted(nd, deg));
+            for (int k = threadIdx.x; k < deg; k += blockDim.x) s.row_eid[b + k] = pb[k];
+        }
+        if (SUM_HERE) {
+            if (threadIdx.x == 0) s.vd[i] = dsqrt(kbn_merge_buf(kb, deg, dmul(4.0, s.nw[i])));
+        } else if (inshm) {
+            for (int k = threadIdx.x; k < deg; k += blockDim.x) slot[k] = kb[k];
+        }
+        __syncthreads();
+    }
+}
+
+template <bool UNIF, bool SUM_HERE>
+__global__ void __launch_bounds__(512) k_edge_block(Sweep s, int begin, int end, int cap)
+{
+    extern __shared__ __align__(16) unsigned char smb[];
+    __shared__ int descents;
+    if (skipped(s)) return;
+    double delta = 0.0;
+    for (int j = begin + blockIdx.x; j < end; j += gridDim.x) {
+        const long long o = s.ioff[j];
+        const int nc = (int)(s.ioff[j + 1] - o);
+        double *slot = s.bkey_e + s.bofs_e[j - s.be0];
+        const bool inshm = nc <= cap;
+        double *kb = inshm ? (double *)smb : slot;
+        int2 *pb = inshm ? (int2 *)((double *)smb + cap) : s.scratch_v + (long long)blockIdx.x * s.scratch_stride;
+        if (threadIdx.x == 0) descents = 0;
+        for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+            int2 pr = s.pairs[o + k];
+            pb[k] = pr;
+            kb[k] = dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
+        }
+        __syncthreads();
+        int d = 0;
+        for (int k = threadIdx.x; k + 1 < nc; k += blockDim.x) d += kb[k + 1] < kb[k];
+        if (d) atomicAdd(&descents, d);
+        __syncthreads();
+        const int nd = descents;
+        if (nd) {
+            fix_order(kb, pb, nc, threadIdx.x, blockDim.x, BlockSync(), BlockAny(), far_from_sorted(nd, nc));
+            for (int k = threadIdx.x; k < nc; k += blockDim.x) s.pairs[o + k] = pb[k];
+        }
+        if (SUM_HERE) {
+            if (threadIdx.x == 0) {
+                const int u = s.eu[j], v = s.ev[j];
+                delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_merge_buf(kb, nc, self_term<UNIF>(s, j, u, v))));
+            }
+        } else if (inshm) {
+            for (int k = threadIdx.x; k < nc; k += blockDim.x) slot[k] = kb[k];
+        }
+        __syncthreads();
+    }
+    if (SUM_HERE) block_max_to(&s.maxd[s.slot], delta);
+}
+
+// one thread per block item: the sequential sum of its sorted slot
+template <bool UNIF>
+__global__ void __launch_bounds__(128) k_vertex_block_sum(Sweep s, int begin, int end)
+{
+    if (skipped(s)) return;
+    const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end) return;
+    const int deg = (int)(s.row_off[i + 1] - s.row_off[i]);
+    s.vd[i] = dsqrt(kbn_merge_buf(s.bkey_v + s.bofs_v[i - s.bv0], deg, dmul(4.0, s.nw[i])));
+}
+
+template <bool UNIF>
+__global__ void __launch_bounds__(128) k_edge_block_sum(Sweep s, int begin, int end)
+{
+    if (skipped(s)) return;
+    const int j = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    double delta = 0.0;
+    if (j < end) {
+        const int u = s.eu[j], v = s.ev[j];
+        const int nc = (int)(s.ioff[j + 1] - s.ioff[j]);
+        delta = finish_edge<UNIF>(s, j, u, v, kbn_merge_buf(s.bkey_e + s.bofs_e[j - s.be0], nc, self_term<UNIF>(s, j, u, v)));
+    }
+    block_max_to(&s.maxd[s.slot], delta);
+}
+
+// ---- launch of one sweep ------------------------------------------------------------
+
+struct Bins {
+    int start[NB + 1];
+    bool has(int b) const { return start[b + 1] > start[b]; }
+    int count(int b) const { return start[b + 1] - start[b]; }
+};
+
+inline unsigned grid_for(long long n, int threads, long long cap_blocks)
+{
+    long long b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap_blocks) b = cap_blocks;
+    return (unsigned)b;
+}
+
+struct LaunchCfg {
+    int sms;
+    int block_cap;                  // BBIG edges: stored terms in shared memory (16 B each)
+    int vblock_cap;                 // BBIG rows: stored terms in shared memory (12 B each)
+    cudaStream_t st, side;          // thread/streamed items on st, block items on side
+    cudaEvent_t fork, join;
+};
+
+constexpr int THR = 128;
+constexpr int MED_THR = 256;
+inline size_t med_smem_vertex() { return (size_t)(MED_THR / 32) * MED_CAP * (8 + 4); }
+inline size_t med_smem_edge() { return (size_t)(MED_THR / 32) * MED_CAP * (8 + 8); }
+
+template <bool UNIF>
+Status set_sweep_attributes(int block_cap, int vblock_cap)
+{
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_block<UNIF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        vblock_cap * 12));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_block<UNIF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        block_cap * 16));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_block<UNIF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        BIG_CAP * 12));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_block<UNIF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        BIG_CAP * 16));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_med_sort<UNIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)med_smem_vertex()));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_med_sort<UNIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)med_smem_edge()));
+    return Status::Ok();
+}
+
+// Block items on the side stream: the largest (one block per SM, full shared
+// memory) first, then the ones up to BIG_CAP terms (several blocks per SM).
+template <bool UNIF, bool EDGE>
+void launch_blocks(const Sweep &s, const Bins &b, const LaunchCfg &c)
+{
+    if (b.has(BBIG)) {
+        if (EDGE)
+            count_launch(), k_edge_block<UNIF, true><<<grid_for(b.count(BBIG), 1, c.sms), 512, (size_t)c.block_cap * 16,
+                                                 c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.block_cap);
+        else
+            count_launch(), k_vertex_block<UNIF, true><<<grid_for(b.count(BBIG), 1, c.sms), 512, (size_t)c.vblock_cap * 12,
+                                                   c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.vblock_cap);
+    }
+    if (b.has(BBLOCK)) {
+        if (EDGE)
+            count_launch(), k_edge_block<UNIF, false><<<grid_for(b.count(BBLOCK), 1, 3 * c.sms), 512, (size_t)BIG_CAP * 16,
+                                                 c.side>>>(s, b.start[BBLOCK], b.start[BBLOCK + 1], BIG_CAP);
+        else
+            count_launch(), k_vertex_block<UNIF, false><<<grid_for(b.count(BBLOCK), 1, 4 * c.sms), 512, (size_t)BIG_CAP * 12,
+                                                   c.side>>>(s, b.start[BBLOCK], b.start[BBLOCK + 1], BIG_CAP);
+    }
+    const int n = b.count(BBLOCK);                       // BBIG items are summed in their block
+    if (n > 0) {
+        const int first = b.start[BBLOCK];
+        if (EDGE) count_launch(), k_edge_block_sum<UNIF><<<grid_for(n, THR, INT_MAX), THR, 0, c.side>>>(s, first, first + n);
+        else count_launch(), k_vertex_block_sum<UNIF><<<grid_for(n, THR, INT_MAX), THR, 0, c.side>>>(s, first, first + n);
+    }
+}
+
+// Streamed items: one pass over all of them, then the queued ones sorted and finished.
+template <bool UNIF, bool EDGE>
+void launch_med(const Sweep &s, const Bins &b, const LaunchCfg &c)
+{
+    if (!b.has(BMED)) return;
+    const unsigned g = grid_for(b.count(BMED), MED_THR, INT_MAX);
+    const unsigned gq = grid_for(b.count(BMED), MED_THR / 32, 8 * c.sms);
+    if (EDGE) {
+        count_launch(), k_edge_med<UNIF><<<g, MED_THR, 0, c.st>>>(s, b.start[BMED], b.start[BMED + 1]);
+        count_launch(), k_edge_med_sort<UNIF><<<gq, MED_THR, med_smem_edge(), c.st>>>(s);
+    } else {
+        count_launch(), k_vertex_med<UNIF><<<g, MED_THR, 0, c.st>>>(s, b.start[BMED], b.start[BMED + 1]);
+        count_launch(), k_vertex_med_sort<UNIF><<<gq, MED_THR, med_smem_vertex(), c.st>>>(s);
+    }
+}
+
+// One sweep: vertex phase, then edge phase.  Within a phase the block items
+// run on the side stream, concurrently with everything else on the main
+// stream; the phase ends when both are done.
+template <bool UNIF>
+Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, const LaunchCfg &c)
+{
+    DRESS_CUDA_TRY(cudaMemsetAsync(s.qcount, 0, 2 * sizeof(unsigned), c.st));
+    const bool vside = vb.has(BBLOCK) || vb.has(BBIG);
+    if (vside) {
+        DRESS_CUDA_TRY(cudaEventRecord(c.fork, c.st));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
+        launch_blocks<UNIF, false>(s, vb, c);
+    }
+    launch_med<UNIF, false>(s, vb, c);
+    if (vb.has(B16)) count_launch(), k_vertex_thr<16, UNIF><<<grid_for(vb.count(B16), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B16], vb.start[B16 + 1]);
+    if (vb.has(B8)) count_launch(), k_vertex_thr<8, UNIF><<<grid_for(vb.count(B8), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B8], vb.start[B8 + 1]);
+    if (vb.has(B4)) count_launch(), k_vertex_thr<4, UNIF><<<grid_for(vb.count(B4), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B4], vb.start[B4 + 1]);
+    if (vb.has(B2)) count_launch(), k_vertex_thr<2, UNIF><<<grid_for(vb.count(B2), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B2], vb.start[B2 + 1]);
+    if (vb.has(B0)) count_launch(), k_vertex_thr<0, UNIF><<<grid_for(vb.count(B0), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B0], vb.start[B0 + 1]);
+    if (vside) {
+        DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
+    }
+    const bool eside = eb.has(BBLOCK) || eb.has(BBIG);
+    if (eside) {
+        DRESS_CUDA_TRY(cudaEventRecord(c.fork, c.st));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
+        launch_blocks<UNIF, true>(s, eb, c);
+    }
+    launch_med<UNIF, true>(s, eb, c);
+    if (eb.has(B16)) count_launch(), k_edge_thr<16, UNIF><<<grid_for(eb.count(B16), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B16], eb.start[B16 + 1]);
+    if (eb.has(B8)) count_launch(), k_edge_thr<8, UNIF><<<grid_for(eb.count(B8), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B8], eb.start[B8 + 1]);
+    if (eb.has(B4)) count_launch(), k_edge_thr<4, UNIF><<<grid_for(eb.count(B4), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B4], eb.start[B4 + 1]);
+    if (eb.has(B2)) count_launch(), k_edge_thr<2, UNIF><<<grid_for(eb.count(B2), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B2], eb.start[B2 + 1]);
+    if (eb.has(B0)) count_launch(), k_edge_thr<0, UNIF><<<grid_for(eb.count(B0), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B0], eb.start[B0 + 1]);
+    if (eside) {
+        DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
+    }
+    DRESS_CUDA_TRY(cudaGetLastError());
+    return Status::Ok();
+}
+
+}  // namespace sweep
+}  // namespace dress
