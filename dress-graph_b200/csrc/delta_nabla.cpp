@@ -175,7 +175,7 @@ Status prepare(Prep &p)
 }
 
 // ---- per-subgraph path ----------------------------------------------------------
-Status run_per_fit(Prep &p)
+Status run_per_fit(Prep &p, const Ctx &ctx)
 {
     dressx_hist_request_t *r = p.r;
     p_dress_graph_t g = p.g;
@@ -258,7 +258,7 @@ Status run_per_fit(Prep &p)
         p_dress_graph_t sub = dress_init_graph(sN, sE, sU, sV, sW, sNW, g->variant, g->precompute_intercepts);
         if (!sub) return Status::Err(DRESSX_EINVAL, "subgraph construction failed");
         FitStats fs;
-        Status st = fit_graph(sub, r->max_iterations, r->epsilon, nullptr, nullptr, &fs);
+        Status st = fit_graph(sub, r->max_iterations, r->epsilon, nullptr, nullptr, &fs, ctx);
         if (!st.ok()) {
             dress_free_graph(sub);
             return st;
@@ -348,10 +348,10 @@ struct BatchPlan {
     float fit_ms = 0.f, hist_ms = 0.f;       // device time of the last run
 };
 
-Status plan_batched(std::vector<Prep *> &ps, Engine &en, BatchPlan &P)
+Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
 {
     P.ps = ps;
-    cudaStream_t st = en.stream;
+    cudaStream_t st = en.st;
     int smem_optin = 0;
     DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, en.device));
     const long long smem_cap = smem_optin - 256;
@@ -390,7 +390,7 @@ Status plan_batched(std::vector<Prep *> &ps, Engine &en, BatchPlan &P)
         nranks += (long long)p->ranks.size();
         if (p->ms_host) ms_total += p->total * (long long)p->E;
     }
-    Tune tu = pick_tune(maxE, maxN, M, en.cfg);
+    Tune tu = pick_tune(maxE, maxN, M, *en.cfg);
     BatchLaunch &L = P.L;
     L.gsize = tu.gsize;
     L.maxE = maxE;
@@ -500,9 +500,9 @@ Status plan_batched(std::vector<Prep *> &ps, Engine &en, BatchPlan &P)
 
 // Device work of a planned batch: all fits, then the histograms (left in
 // device memory).  Can be repeated; each run starts from the same inputs.
-Status exec_batched(BatchPlan &P, Engine &en)
+Status exec_batched(BatchPlan &P, const Ctx &en)
 {
-    cudaStream_t st = en.stream;
+    cudaStream_t st = en.st;
     const int nreq = (int)P.ps.size();
     DRESS_CUDA_TRY(cudaMemsetAsync(P.d_stats.get(), 0, 4 * (size_t)nreq * sizeof(unsigned long long), st));
     DRESS_CUDA_TRY(cudaMemsetAsync(P.d_counter.get(), 0, sizeof(int), st));
@@ -532,9 +532,9 @@ Status exec_batched(BatchPlan &P, Engine &en)
 }
 
 // Results of the last run into the requests' host-side state.
-Status collect_batched(BatchPlan &P, Engine &en)
+Status collect_batched(BatchPlan &P, const Ctx &en)
 {
-    cudaStream_t st = en.stream;
+    cudaStream_t st = en.st;
     const int nreq = (int)P.ps.size();
     std::vector<Prep *> &ps = P.ps;
     for (int i = 0; i < nreq; ++i) {
@@ -561,7 +561,7 @@ Status collect_batched(BatchPlan &P, Engine &en)
     return Status::Ok();
 }
 
-Status run_batched(std::vector<Prep *> &ps, Engine &en)
+Status run_batched(std::vector<Prep *> &ps, const Ctx &en)
 {
     BatchPlan P;
     DRESS_TRY(plan_batched(ps, en, P));
@@ -586,12 +586,12 @@ Status finish(Prep &p)
     return Status::Ok();
 }
 
-Status hist_batch_impl(dressx_hist_request_t *reqs, int n, bool per_fit)
+}  // namespace
+
+// All requests on one execution context (no locking: the caller owns ctx).
+Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const Ctx &ctx)
 {
-    Engine &en = engine();
-    std::lock_guard<std::mutex> lk(en.mu);
-    DRESS_TRY(en.init());
-    DRESS_CUDA_TRY(cudaSetDevice(en.device));
+    DRESS_CUDA_TRY(cudaSetDevice(ctx.device));
     std::vector<Prep> ps((size_t)n);
     Status first;
     for (int i = 0; i < n; ++i) {
@@ -613,7 +613,7 @@ Status hist_batch_impl(dressx_hist_request_t *reqs, int n, bool per_fit)
         if (p.inplace) {
             // k == 0: fit the caller's graph itself (libdress/src/delta_dress_impl.c:206-224)
             FitStats fs;
-            Status s = fit_graph(p.g, p.r->max_iterations, p.r->epsilon, nullptr, nullptr, &fs);
+            Status s = fit_graph(p.g, p.r->max_iterations, p.r->epsilon, nullptr, nullptr, &fs, ctx);
             if (!s.ok()) { p.r->status = s.code; if (first.ok()) first = s; continue; }
             for (int e = 0; e < p.E; ++e) {
                 long long b;
@@ -628,13 +628,13 @@ Status hist_batch_impl(dressx_hist_request_t *reqs, int n, bool per_fit)
         } else if (p.batchable && !per_fit) {
             batch.push_back(&p);
         } else {
-            Status s = run_per_fit(p);
+            Status s = run_per_fit(p, ctx);
             if (!s.ok()) { p.r->status = s.code; if (first.ok()) first = s; continue; }
             host_vals.push_back(&p);
         }
     }
     if (!batch.empty()) {
-        Status s = run_batched(batch, en);
+        Status s = run_batched(batch, ctx);
         if (!s.ok()) {
             for (Prep *p : batch) p->r->status = s.code;
             if (first.ok()) first = s;
@@ -644,7 +644,7 @@ Status hist_batch_impl(dressx_hist_request_t *reqs, int n, bool per_fit)
         std::vector<Prep *> hv;
         for (Prep *p : host_vals)
             if (p->r->want_histogram) hv.push_back(p);
-        Status s = hist_of_host_values(hv, en.stream, en.num_sms);
+        Status s = hist_of_host_values(hv, ctx.st, ctx.num_sms);
         if (!s.ok()) {
             for (Prep *p : hv) p->r->status = s.code;
             if (first.ok()) first = s;
@@ -658,6 +658,16 @@ Status hist_batch_impl(dressx_hist_request_t *reqs, int n, bool per_fit)
         if (p.ms_host) { std::free(p.ms_host); p.ms_host = nullptr; }
     }
     return first;
+}
+
+namespace {
+
+Status hist_batch_impl(dressx_hist_request_t *reqs, int n, bool per_fit)
+{
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    DRESS_TRY(en.init());
+    return hist_batch_core(reqs, n, per_fit, en.ctx);
 }
 
 // ---- legacy wrappers -------------------------------------------------------------------
@@ -838,7 +848,7 @@ Status batch_create(dressx_hist_request_t *reqs, int n, dressx_batch_t **out)
         if (!p.empty) b->ptrs.push_back(&p);
     }
     if (!b->ptrs.empty()) {
-        Status s = plan_batched(b->ptrs, en, b->plan);
+        Status s = plan_batched(b->ptrs, en.ctx, b->plan);
         if (!s.ok()) {
             for (auto &q : b->preps) std::free(q.ms_host);
             delete b;
@@ -867,7 +877,7 @@ int dressx_batch_run(dressx_batch_t *b)
     if (!b) return DRESSX_EINVAL;
     Engine &en = engine();
     std::lock_guard<std::mutex> lk(en.mu);
-    Status s = b->ptrs.empty() ? Status::Ok() : exec_batched(b->plan, en);
+    Status s = b->ptrs.empty() ? Status::Ok() : exec_batched(b->plan, en.ctx);
     b->ran = s.ok();
     set_last_error(s);
     return s.code;
@@ -878,7 +888,7 @@ int dressx_batch_fetch(dressx_batch_t *b)
     if (!b || !b->ran) return DRESSX_EINVAL;
     Engine &en = engine();
     std::lock_guard<std::mutex> lk(en.mu);
-    Status s = b->ptrs.empty() ? Status::Ok() : collect_batched(b->plan, en);
+    Status s = b->ptrs.empty() ? Status::Ok() : collect_batched(b->plan, en.ctx);
     for (auto &p : b->preps) {
         if (!s.ok()) break;
         std::free(p.r->hist_flat);
@@ -930,7 +940,7 @@ void dressx_batch_destroy(dressx_batch_t *b)
     std::lock_guard<std::mutex> lk(en.mu);
     for (auto &p : b->preps) std::free(p.ms_host);
     delete b;
-    cudaStreamSynchronize(en.stream);
+    cudaStreamSynchronize(en.ctx.st);
 }
 
 }  // extern "C"

@@ -48,18 +48,39 @@ Status Pinned::reserve(size_t bytes)
     return Status::Ok();
 }
 
+Status Ctx::create(int dev, int sms, const dressx_config_t *config)
+{
+    device = dev;
+    num_sms = sms;
+    cfg = config;
+    DRESS_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    DRESS_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    DRESS_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    return Status::Ok();
+}
+
+void Ctx::destroy()
+{
+    if (st) cudaStreamSynchronize(st);
+    if (side) cudaStreamSynchronize(side);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (st) cudaStreamDestroy(st);
+    if (side) cudaStreamDestroy(side);
+    st = side = nullptr;
+    fork = join = nullptr;
+}
+
 Status Engine::init()
 {
-    if (stream) return Status::Ok();
+    if (ctx.st) return Status::Ok();
     int dev = cfg.device;
     if (dev < 0) DRESS_CUDA_TRY(cudaGetDevice(&dev));
     DRESS_CUDA_TRY(cudaSetDevice(dev));
     device = dev;
     DRESS_CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
-    DRESS_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    DRESS_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
-    DRESS_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-    DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    DRESS_TRY(ctx.create(dev, num_sms, &cfg));
     cudaMemPool_t pool;
     DRESS_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
     unsigned long long keep = cfg.memory_budget_bytes ? cfg.memory_budget_bytes : ~0ULL;
@@ -80,7 +101,7 @@ Status fit_locked(p_dress_graph_t g, int max_iterations, double epsilon, int *it
     DRESS_TRY(en.init());
     DRESS_CUDA_TRY(cudaSetDevice(en.device));
     FitStats st;
-    Status s = fit_graph(g, max_iterations, epsilon, iterations, delta, &st);
+    Status s = fit_graph(g, max_iterations, epsilon, iterations, delta, &st, en.ctx);
     if (s.ok()) g_last_stats = st;
     return s;
 }
@@ -96,7 +117,7 @@ int dressx_configure(const dressx_config_t *cfg)
     Engine &en = engine();
     std::lock_guard<std::mutex> lk(en.mu);
     if (!cfg) return DRESSX_EINVAL;
-    if (en.stream && cfg->device >= 0 && cfg->device != en.device) {
+    if (en.ctx.st && cfg->device >= 0 && cfg->device != en.device) {
         set_last_error(Status::Err(DRESSX_EINVAL, "engine already bound to another device"));
         return DRESSX_EINVAL;
     }
@@ -150,7 +171,7 @@ int dressx_stream(void **stream)
     std::lock_guard<std::mutex> lk(en.mu);
     Status s = en.init();
     set_last_error(s);
-    *stream = s.ok() ? (void *)en.stream : nullptr;
+    *stream = s.ok() ? (void *)en.ctx.st : nullptr;
     return s.code;
 }
 
@@ -158,10 +179,14 @@ int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, i
 {
     Engine &en = engine();
     std::lock_guard<std::mutex> lk(en.mu);
-    if (h2d_bytes) *h2d_bytes = en.h2d_bytes;
-    if (d2h_bytes) *d2h_bytes = en.d2h_bytes;
-    if (launches) *launches = en.launches;
-    if (reset) en.h2d_bytes = en.d2h_bytes = en.launches = 0;
+    if (h2d_bytes) *h2d_bytes = en.h2d_bytes.load();
+    if (d2h_bytes) *d2h_bytes = en.d2h_bytes.load();
+    if (launches) *launches = en.launches.load();
+    if (reset) {
+        en.h2d_bytes = 0;
+        en.d2h_bytes = 0;
+        en.launches = 0;
+    }
     return DRESSX_OK;
 }
 

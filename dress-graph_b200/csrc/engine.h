@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -87,18 +88,30 @@ class Pinned {
     size_t cap_ = 0;
 };
 
+// ---- an execution context: where one stream of work runs ------------------
+// The legacy entry points share the engine's context; every server lane owns
+// one, so lanes keep independent work in flight on the device at once.
+struct Ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t st = nullptr;             // main stream
+    cudaStream_t side = nullptr;           // concurrent hub work of the single-graph fit
+    cudaEvent_t fork = nullptr, join = nullptr;
+    const dressx_config_t *cfg = nullptr;
+    Status create(int dev, int sms, const dressx_config_t *config);
+    void destroy();
+};
+
 // ---- the per-process engine ------------------------------------------------
 struct Engine {
     int device = -1;
-    cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;           // second stream for overlapped bins
-    cudaEvent_t fork = nullptr, join = nullptr;
+    Ctx ctx;                               // context of the legacy entry points
     std::mutex mu;                         // legacy entry points are serialised
     Pinned pinned;
     int num_sms = 148;
     dressx_config_t cfg;
     // traffic and launch counters of the public calls (reset by the caller)
-    long long h2d_bytes = 0, d2h_bytes = 0, launches = 0;
+    std::atomic<long long> h2d_bytes{0}, d2h_bytes{0}, launches{0};
     Status init();
 };
 
@@ -131,6 +144,9 @@ struct FitStats {
     double setup_ms = 0, iterate_ms = 0;
 };
 Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon,
-                 int *iterations, double *delta, FitStats *stats);
+                 int *iterations, double *delta, FitStats *stats, const Ctx &ctx);
+
+// ---- Delta/Nabla requests (delta_nabla.cpp) ---------------------------------
+Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const Ctx &ctx);
 
 }  // namespace dress

@@ -325,7 +325,7 @@ double ms_since(std::chrono::steady_clock::time_point t0)
 }  // namespace
 
 Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *iterations,
-                 double *delta, FitStats *stats)
+                 double *delta, FitStats *stats, const Ctx &ctx)
 {
     auto t0 = std::chrono::steady_clock::now();
     if (!g) return Status::Err(DRESSX_EINVAL, "graph is NULL");
@@ -343,9 +343,8 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     const long long S = N > 0 ? g->adj_offset[N] : 0;
     if (N > 0 && (g->adj_offset[0] != 0 || S < 0)) return Status::Err(DRESSX_EINVAL, "bad adj_offset");
 
-    Engine &en = engine();
-    cudaStream_t st = en.stream;
-    const int sms = en.num_sms;
+    cudaStream_t st = ctx.st;
+    const int sms = ctx.num_sms;
     const int fwd = (g->variant == DRESS_VARIANT_FORWARD || g->variant == DRESS_VARIANT_BACKWARD);
 
     // ---- upload --------------------------------------------------------
@@ -568,7 +567,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
 
     // block-bin shared memory and spill area
     int smem_optin = 0;
-    DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, en.device));
+    DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx.device));
     // keys (8 B) and payload (8 B edge pair, 4 B row slot) per stored term,
     // leaving room for static shared memory
     int block_cap = (smem_optin - 1024) / 16;
@@ -617,7 +616,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     s.bkey_v = d_bkey_v.get(); s.bkey_e = d_bkey_e.get();
     s.bofs_v = d_bofs_v.get(); s.bofs_e = d_bofs_e.get();
     s.bv0 = vb.start[BBLOCK]; s.be0 = eb.start[BBLOCK];
-    LaunchCfg lc{sms, block_cap, vblock_cap, st, en.side, en.fork, en.join};
+    LaunchCfg lc{sms, block_cap, vblock_cap, st, ctx.side, ctx.fork, ctx.join};
     double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + E};
     double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + E};
 
@@ -625,7 +624,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     // first, and the first sweep of a chunk still sees the previous slot
     unsigned long long hmax[RING];
     int conv = -1, done = 0;
-    int chunk = en.cfg.fit_chunk > 0 ? (en.cfg.fit_chunk < MAX_CHUNK ? en.cfg.fit_chunk : MAX_CHUNK) : 8;
+    int chunk = ctx.cfg->fit_chunk > 0 ? (ctx.cfg->fit_chunk < MAX_CHUNK ? ctx.cfg->fit_chunk : MAX_CHUNK) : 8;
     double last_delta = 0.0;
     while (done < max_iterations && conv < 0) {
         int hi = done + chunk < max_iterations ? done + chunk : max_iterations;
