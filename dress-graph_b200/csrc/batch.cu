@@ -166,12 +166,12 @@ __device__ __forceinline__ int group_sum(const Group &g, int v, double *red, int
 }
 
 template <int M>
-__device__ void fit_item(const BatchLaunch &L, const ParentDesc &P, const View &G, long long item,
+__device__ void fit_item(const ParentDesc &P, const View &G, long long item,
                          const Group &g, double *d0, double *d1, double *vd, double *red, int *ks,
                          unsigned long long *slot)
 {
     const int N = P.N, E = P.E;
-    const long long s = P.ranks_off >= 0 ? L.ranks[P.ranks_off + item] : P.offset + item * P.stride;
+    const long long s = P.ranks ? P.ranks[item] : P.offset + item * P.stride;
     // ---- unrank the subset / tuple --------------------------------------
     if (g.t == 0 && P.kind != ITEM_PLAIN) {
         long long r = s;
@@ -211,13 +211,14 @@ __device__ void fit_item(const BatchLaunch &L, const ParentDesc &P, const View &
         d0[e] = P.has_dinit ? G.dinit[e] : 1.0;
     }
     live = group_sum(g, live, red, 0);
-    if (live == 0) {            // the reference skips edgeless subgraphs
+    if (live == 0 && P.kind != ITEM_PLAIN) {   // the reference skips edgeless subgraphs
         g.sync();
         return;
     }
 
     // ---- sweeps ------------------------------------------------------------------
     int it = 0;
+    double last = 0.0;
     for (; it < P.max_iter; ++it) {
         for (int u = g.t; u < N; u += g.size) {
             if (!mk.alive(u)) continue;
@@ -267,6 +268,7 @@ __device__ void fit_item(const BatchLaunch &L, const ParentDesc &P, const View &
             if (dd > lmax) lmax = dd;
         }
         const double m = group_max(g, lmax, red, (it & 1));
+        last = m;
         double *t = d0;
         d0 = d1;
         d1 = t;
@@ -275,22 +277,40 @@ __device__ void fit_item(const BatchLaunch &L, const ParentDesc &P, const View &
     }
     const int sweeps = it < P.max_iter ? it + 1 : P.max_iter;
 
+    // ---- plain fit: the final state in edge / vertex order -------------------------
+    if (P.kind == ITEM_PLAIN) {
+        for (int e = g.t; e < E; e += g.size) P.values[e] = d0[e];
+        if (P.max_iter > 0)     // the norms of the last sweep (none without sweeps)
+            for (int u = g.t; u < N; u += g.size) P.values[E + u] = vd[u];
+        if (g.t == 0) {
+            unsigned long long *st = P.stats;
+            const int done = P.max_iter > 0 ? sweeps : 0;
+            st[ST_SWEEPS] = (unsigned long long)done;
+            st[ST_EDGE_ITERS] = (unsigned long long)E * (unsigned long long)done;
+            st[ST_FITS] = 1ULL;
+            st[ST_ITERATIONS] = (unsigned long long)(it < P.max_iter ? it : P.max_iter);
+            st[ST_DELTA] = (unsigned long long)__double_as_longlong(last);
+        }
+        g.sync();
+        return;
+    }
+
     // ---- emit the live values -------------------------------------------------------
     if (g.t == 0) {
-        slot[0] = atomicAdd(&L.cursors[P.req], (unsigned long long)live);
+        slot[0] = atomicAdd(&P.stats[ST_CURSOR], (unsigned long long)live);
         slot[1] = 0;
-        atomicAdd(&L.sweeps[P.req], (unsigned long long)sweeps);
-        atomicAdd(&L.edge_iters[P.req], (unsigned long long)live * (unsigned long long)sweeps);
-        atomicAdd(&L.fits[P.req], 1ULL);
+        atomicAdd(&P.stats[ST_SWEEPS], (unsigned long long)sweeps);
+        atomicAdd(&P.stats[ST_EDGE_ITERS], (unsigned long long)live * (unsigned long long)sweeps);
+        atomicAdd(&P.stats[ST_FITS], 1ULL);
     }
     g.sync();
-    const long long base = P.val_base + (long long)slot[0];
-    double *row = P.ms_base >= 0 ? L.multisets + P.ms_base + s * P.E_ms : nullptr;
+    double *out = P.values + (long long)slot[0];
+    double *row = P.multisets ? P.multisets + s * (long long)E : nullptr;
     for (int e = g.t; e < E; e += g.size) {
         bool al = mk.alive(G.U[e]) && mk.alive(G.V[e]);
         if (al) {
             unsigned long long q = atomicAdd(&slot[1], 1ULL);
-            L.values[base + (long long)q] = d0[e];
+            out[q] = d0[e];
         }
         if (row) row[e] = al ? d0[e] : __longlong_as_double(0x7ff8000000000000LL);
     }
@@ -303,8 +323,29 @@ __host__ __device__ inline long long group_bytes(const BatchLaunch &L)
     return pl_align(b);
 }
 
-template <int M>
-__global__ void __launch_bounds__(512, 1) k_batch(BatchLaunch L)
+__device__ __forceinline__ View view_of(const unsigned char *b, const ParentLayout &PL, const ParentDesc &P)
+{
+    View G;
+    G.U = (const int *)(b + PL.U);
+    G.V = (const int *)(b + PL.V);
+    G.w = (const double *)(b + PL.w);
+    G.row_off = (const int *)(b + PL.row_off);
+    G.row_eid = (const int *)(b + PL.row_eid);
+    G.ioff = (const int *)(b + PL.ioff);
+    G.pairs = (const int2 *)(b + PL.pairs);
+    G.nw = P.has_nw ? (const double *)(b + PL.nw) : nullptr;
+    G.dinit = P.has_dinit ? (const double *)(b + PL.dinit) : nullptr;
+    return G;
+}
+
+// Two schedules.  CTA mode: the CTA takes a chunk, stages its parent in
+// shared memory and its groups share the chunk's subgraphs.  Group mode
+// (whole-graph fits, one item per chunk): every group takes chunks on its
+// own and reads the parent through L2, so no group idles behind another.
+// Group-mode CTAs hold at most 256 threads (several per SM), which leaves
+// the register budget of the larger networks unsplit.
+template <int M, bool GROUP>
+__global__ void __launch_bounds__(GROUP ? 256 : 512, 1) k_batch(BatchLaunch L)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_chunk, s_next;
@@ -317,6 +358,21 @@ __global__ void __launch_bounds__(512, 1) k_batch(BatchLaunch L)
     double *red = vd + L.maxN;
     unsigned long long *slot = (unsigned long long *)(red + 2 * (L.gsize / 32));
     int *ks = (int *)(slot + 2);
+    if (GROUP) {
+        for (;;) {
+            if (g.t == 0) slot[0] = (unsigned long long)atomicAdd(L.chunk_counter, 1);
+            g.sync();
+            const int c = (int)slot[0];
+            g.sync();
+            if (c >= L.nchunks) break;
+            const Chunk ch = L.chunks[c];
+            const ParentDesc P = L.parents[ch.parent];
+            const ParentLayout PL = parent_layout(P.N, P.E, P.S, P.T, P.has_nw, P.has_dinit);
+            const View G = view_of(P.data, PL, P);
+            for (int i = 0; i < ch.count; ++i) fit_item<M>(P, G, ch.first + i, g, d0, d1, vd, red, ks, slot);
+        }
+        return;
+    }
     int staged = -1;
     for (;;) {
         if (threadIdx.x == 0) s_chunk = atomicAdd(L.chunk_counter, 1);
@@ -327,49 +383,49 @@ __global__ void __launch_bounds__(512, 1) k_batch(BatchLaunch L)
         const ParentDesc P = L.parents[ch.parent];
         const ParentLayout PL = parent_layout(P.N, P.E, P.S, P.T, P.has_nw, P.has_dinit);
         if (L.stage && ch.parent != staged) {
-            const int4 *src = (const int4 *)(L.pdata + P.data_off);
+            const int4 *src = (const int4 *)P.data;
             int4 *dst = (int4 *)smem;
             for (long long q = threadIdx.x; q < PL.bytes / 16; q += blockDim.x) dst[q] = src[q];
             staged = ch.parent;
         }
         if (threadIdx.x == 0) s_next = 0;
         __syncthreads();
-        const unsigned char *b = L.stage ? smem : L.pdata + P.data_off;
-        View G;
-        G.U = (const int *)(b + PL.U);
-        G.V = (const int *)(b + PL.V);
-        G.w = (const double *)(b + PL.w);
-        G.row_off = (const int *)(b + PL.row_off);
-        G.row_eid = (const int *)(b + PL.row_eid);
-        G.ioff = (const int *)(b + PL.ioff);
-        G.pairs = (const int2 *)(b + PL.pairs);
-        G.nw = P.has_nw ? (const double *)(b + PL.nw) : nullptr;
-        G.dinit = P.has_dinit ? (const double *)(b + PL.dinit) : nullptr;
+        const View G = view_of(L.stage ? smem : P.data, PL, P);
         for (;;) {
             if (g.t == 0) slot[0] = (unsigned long long)atomicAdd(&s_next, 1);
             g.sync();
             const int item = (int)slot[0];
             g.sync();
             if (item >= ch.count) break;
-            fit_item<M>(L, P, G, ch.first + item, g, d0, d1, vd, red, ks, slot);
+            fit_item<M>(P, G, ch.first + item, g, d0, d1, vd, red, ks, slot);
         }
         __syncthreads();
     }
 }
 
+template <int M, bool GROUP>
+Status launch_mg(const BatchLaunch &L, int sms, cudaStream_t st)
+{
+    if (GROUP && L.gsize * L.groups > 256)
+        return Status::Err(DRESSX_EINVAL, "group-mode batch CTAs hold at most 256 threads");
+    size_t smem = batch_smem_bytes(L);
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_batch<M, GROUP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    DRESS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<M, GROUP>, L.gsize * L.groups, smem));
+    if (per_sm < 1) return Status::Err(DRESSX_EUNSUPPORTED, "batch kernel does not fit on an SM");
+    long long grid = (long long)per_sm * sms;
+    // no more CTAs than there are chunks (group mode: chunks per CTA = groups)
+    long long need = GROUP ? (L.nchunks + L.groups - 1) / L.groups : L.nchunks;
+    if (grid > need) grid = need;
+    count_launch(), k_batch<M, GROUP><<<(int)grid, L.gsize * L.groups, smem, st>>>(L);
+    DRESS_CUDA_TRY(cudaGetLastError());
+    return Status::Ok();
+}
+
 template <int M>
 Status launch_m(const BatchLaunch &L, int sms, cudaStream_t st)
 {
-    size_t smem = batch_smem_bytes(L);
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_batch<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    DRESS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<M>, L.gsize * L.groups, smem));
-    if (per_sm < 1) return Status::Err(DRESSX_EUNSUPPORTED, "batch kernel does not fit on an SM");
-    int grid = per_sm * sms;
-    if (grid > L.nchunks) grid = L.nchunks;
-    count_launch(), k_batch<M><<<grid, L.gsize * L.groups, smem, st>>>(L);
-    DRESS_CUDA_TRY(cudaGetLastError());
-    return Status::Ok();
+    return L.per_group ? launch_mg<M, true>(L, sms, st) : launch_mg<M, false>(L, sms, st);
 }
 
 }  // namespace

@@ -34,7 +34,12 @@ __host__ __device__ inline ParentLayout parent_layout(int N, int E, int S, int T
     return L;
 }
 
-// One parent graph of a launch and the subgraphs to fit on it.
+// Per-request statistics record written by the kernel.
+enum { ST_CURSOR = 0, ST_SWEEPS, ST_EDGE_ITERS, ST_FITS, ST_ITERATIONS, ST_DELTA, ST_WORDS };
+
+// One parent graph of a launch and the subgraphs to fit on it.  Every
+// pointer addresses device memory owned by the request, so requests of one
+// launch may live in unrelated allocations.
 struct ParentDesc {
     int N, E, S, T;
     int kind;            // ITEM_*
@@ -43,14 +48,13 @@ struct ParentDesc {
     int max_iter;
     double eps;
     int has_nw, has_dinit;
-    int req;             // request slot (value cursor, statistics)
-    int pad;
-    long long data_off;  // byte offset of the packed arrays in the parent arena
-    long long offset, stride;   // rank of item i = offset + i*stride ...
-    long long ranks_off; // ... or ranks[ranks_off + i] when >= 0 (sampling)
-    long long val_base;  // first slot of this request's value segment
-    long long ms_base;   // multiset matrix of this request, -1 = none
-    long long E_ms;      // row length of the multiset matrix
+    const unsigned char *data;   // packed arrays (parent_layout)
+    double *values;      // DELTA/NABLA: live values in completion order;
+                         // PLAIN: E final edge values, then N vertex norms
+    unsigned long long *stats;   // ST_WORDS counters
+    double *multisets;   // C(N,k) x E row-major matrix, or null
+    const long long *ranks;      // sampled ranks (item i -> ranks[i]), or null ...
+    long long offset, stride;    // ... else rank of item i = offset + i*stride
 };
 
 struct Chunk {
@@ -61,19 +65,12 @@ struct Chunk {
 
 struct BatchLaunch {
     const ParentDesc *parents;
-    const unsigned char *pdata;
     const Chunk *chunks;
     int nchunks;
     int *chunk_counter;
-    const long long *ranks;
-    double *values;
-    unsigned long long *cursors;     // per request: values written
-    unsigned long long *sweeps;      // per request: sum of sweeps over fits
-    unsigned long long *edge_iters;  // per request: sum of live edges x sweeps
-    unsigned long long *fits;        // per request: subgraphs fitted
-    double *multisets;
     int gsize, groups;               // threads per subgraph, subgraphs per CTA
-    int stage;                       // parents copied into shared memory
+    int stage;                       // parents copied into shared memory (CTA mode)
+    int per_group;                   // every group takes its own chunks (no staging)
     int maxE, maxN, maxk;            // per-group state sizes
     long long parent_bytes;          // staging area size
     int M;                           // register network size (max terms)

@@ -361,6 +361,9 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
     long long maxbytes = 16, arena = 0, values = 0, ms_total = 0, nranks = 0;
     std::vector<ParentDesc> &descs = P.descs;
     std::vector<long long> &val_base = P.val_base;
+    // byte / element offsets of each request's sections, turned into device
+    // pointers once the buffers exist
+    std::vector<long long> data_off, ranks_off, ms_off;
     for (Prep *p : ps) {
         ParentLayout PL = parent_layout(p->N, p->E, p->S, p->T, 0, 0);
         maxE = std::max(maxE, p->E);
@@ -375,14 +378,11 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
         d.fwd = p->g->variant == DRESS_VARIANT_FORWARD || p->g->variant == DRESS_VARIANT_BACKWARD;
         d.max_iter = p->r->max_iterations;
         d.eps = p->r->epsilon;
-        d.req = (int)descs.size();
-        d.data_off = arena;
         d.offset = p->r->offset;
         d.stride = p->r->stride;
-        d.ranks_off = p->ranks.empty() ? -1 : nranks;
-        d.val_base = values;
-        d.ms_base = p->ms_host ? ms_total : -1;
-        d.E_ms = p->E;
+        data_off.push_back(arena);
+        ranks_off.push_back(p->ranks.empty() ? -1 : nranks);
+        ms_off.push_back(p->ms_host ? ms_total : -1);
         descs.push_back(d);
         val_base.push_back(values);
         arena += PL.bytes;
@@ -426,7 +426,7 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
         Prep *p = ps[i];
         p_dress_graph_t g = p->g;
         ParentLayout PL = parent_layout(p->N, p->E, p->S, p->T, 0, 0);
-        unsigned char *b = hbytes.data() + descs[i].data_off;
+        unsigned char *b = hbytes.data() + data_off[i];
         std::memcpy(b + PL.U, g->U, (size_t)p->E * 4);
         std::memcpy(b + PL.V, g->V, (size_t)p->E * 4);
         std::memcpy(b + PL.w, g->edge_weight, (size_t)p->E * 8);
@@ -458,9 +458,17 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
     DRESS_TRY(d_chunks.alloc(chunks.size(), st));
     DRESS_TRY(d_ranks.alloc(hranks.size() + 1, st));
     DRESS_TRY(d_vals.alloc((size_t)values + 1, st));
-    DRESS_TRY(d_stats.alloc(4 * (size_t)nreq, st));
+    DRESS_TRY(d_stats.alloc(ST_WORDS * (size_t)nreq, st));
     DRESS_TRY(d_counter.alloc(1, st));
     if (ms_total > 0) DRESS_TRY(d_ms.alloc((size_t)ms_total, st));
+    for (int i = 0; i < nreq; ++i) {
+        ParentDesc &d = descs[(size_t)i];
+        d.data = d_pdata.get() + data_off[(size_t)i];
+        d.values = (double *)d_vals.get() + val_base[(size_t)i];
+        d.stats = d_stats.get() + ST_WORDS * (size_t)i;
+        d.multisets = ms_off[(size_t)i] >= 0 ? d_ms.get() + ms_off[(size_t)i] : nullptr;
+        d.ranks = ranks_off[(size_t)i] >= 0 ? d_ranks.get() + ranks_off[(size_t)i] : nullptr;
+    }
     DRESS_CUDA_TRY(counted_memcpy(d_pdata.get(), hbytes.data(), (size_t)arena, cudaMemcpyHostToDevice, st));
     DRESS_CUDA_TRY(counted_memcpy(d_desc.get(), descs.data(), descs.size() * sizeof(ParentDesc),
                                    cudaMemcpyHostToDevice, st));
@@ -481,17 +489,10 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
             }
     }
     L.parents = d_desc.get();
-    L.pdata = d_pdata.get();
     L.chunks = d_chunks.get();
     L.nchunks = (int)chunks.size();
     L.chunk_counter = d_counter.get();
-    L.ranks = d_ranks.get();
-    L.values = (double *)d_vals.get();
-    L.cursors = d_stats.get();
-    L.sweeps = d_stats.get() + nreq;
-    L.edge_iters = d_stats.get() + 2 * nreq;
-    L.fits = d_stats.get() + 3 * nreq;
-    L.multisets = d_ms.get();
+    L.per_group = 0;
     P.need_hist = false;
     for (Prep *p : ps) P.need_hist |= p->r->want_histogram != 0;
     if (P.need_hist) DRESS_TRY(P.d_alt.alloc((size_t)values + 1, st));
@@ -504,14 +505,14 @@ Status exec_batched(BatchPlan &P, const Ctx &en)
 {
     cudaStream_t st = en.st;
     const int nreq = (int)P.ps.size();
-    DRESS_CUDA_TRY(cudaMemsetAsync(P.d_stats.get(), 0, 4 * (size_t)nreq * sizeof(unsigned long long), st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(P.d_stats.get(), 0, ST_WORDS * (size_t)nreq * sizeof(unsigned long long), st));
     DRESS_CUDA_TRY(cudaMemsetAsync(P.d_counter.get(), 0, sizeof(int), st));
     cudaEvent_t ev[3];
     for (auto &e : ev) DRESS_CUDA_TRY(cudaEventCreate(&e));
     DRESS_CUDA_TRY(cudaEventRecord(ev[0], st));
     DRESS_TRY(launch_batch(P.L, en.num_sms, st));
     DRESS_CUDA_TRY(cudaEventRecord(ev[1], st));
-    P.stats.assign(4 * (size_t)nreq, 0);
+    P.stats.assign(ST_WORDS * (size_t)nreq, 0);
     DRESS_CUDA_TRY(counted_memcpy(P.stats.data(), P.d_stats.get(), P.stats.size() * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -519,7 +520,7 @@ Status exec_batched(BatchPlan &P, const Ctx &en)
         std::vector<long long> begin((size_t)nreq), len((size_t)nreq);
         for (int i = 0; i < nreq; ++i) {
             begin[(size_t)i] = P.val_base[(size_t)i];
-            len[(size_t)i] = (long long)P.stats[(size_t)i];
+            len[(size_t)i] = (long long)P.stats[ST_WORDS * (size_t)i + ST_CURSOR];
         }
         DRESS_TRY(histogram_device(P.d_vals.get(), P.d_alt.get(), begin, len, P.hist, st, en.num_sms));
     }
@@ -538,9 +539,10 @@ Status collect_batched(BatchPlan &P, const Ctx &en)
     const int nreq = (int)P.ps.size();
     std::vector<Prep *> &ps = P.ps;
     for (int i = 0; i < nreq; ++i) {
-        ps[(size_t)i]->sweeps = P.stats[(size_t)nreq + i];
-        ps[(size_t)i]->edge_iters = P.stats[2 * (size_t)nreq + i];
-        ps[(size_t)i]->fits = P.stats[3 * (size_t)nreq + i];
+        const unsigned long long *st_i = P.stats.data() + ST_WORDS * (size_t)i;
+        ps[(size_t)i]->sweeps = st_i[ST_SWEEPS];
+        ps[(size_t)i]->edge_iters = st_i[ST_EDGE_ITERS];
+        ps[(size_t)i]->fits = st_i[ST_FITS];
     }
     if (P.need_hist) {
         std::vector<std::vector<long long>> out;
@@ -915,9 +917,9 @@ int dressx_batch_stats(dressx_batch_t *b, int64_t *fits, int64_t *sweeps, int64_
     long long f = 0, sw = 0, eu = 0;
     const size_t n = b->ptrs.size();
     for (size_t i = 0; i < n && b->plan.stats.size() >= 4 * n; ++i) {
-        sw += (long long)b->plan.stats[n + i];
-        eu += (long long)b->plan.stats[2 * n + i];
-        f += (long long)b->plan.stats[3 * n + i];
+        sw += (long long)b->plan.stats[ST_WORDS * (size_t)i + ST_SWEEPS];
+        eu += (long long)b->plan.stats[ST_WORDS * (size_t)i + ST_EDGE_ITERS];
+        f += (long long)b->plan.stats[ST_WORDS * (size_t)i + ST_FITS];
     }
     if (fits) *fits = f;
     if (sweeps) *sweeps = sw;
