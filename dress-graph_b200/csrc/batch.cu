@@ -430,6 +430,16 @@ Status launch_m(const BatchLaunch &L, int sms, cudaStream_t st)
 
 }  // namespace
 
+long long batch_group_bytes(int maxE, int maxN, int maxk, int gsize)
+{
+    BatchLaunch L{};
+    L.maxE = maxE;
+    L.maxN = maxN;
+    L.maxk = maxk;
+    L.gsize = gsize;
+    return group_bytes(L);
+}
+
 size_t batch_smem_bytes(const BatchLaunch &L)
 {
     return (size_t)((L.stage ? pl_align(L.parent_bytes) : 0) + group_bytes(L) * L.groups);

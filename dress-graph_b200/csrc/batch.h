@@ -2,6 +2,8 @@
 #pragma once
 #include <stdint.h>
 
+#include <vector>
+
 #include "engine.h"
 
 namespace dress {
@@ -78,5 +80,19 @@ struct BatchLaunch {
 
 Status launch_batch(const BatchLaunch &L, int sms, cudaStream_t st);
 size_t batch_smem_bytes(const BatchLaunch &L);
+// Shared memory of one group's state (edge values twice, vertex norms,
+// reduction slots, the k mask vertices); a graph is batchable only when one
+// group fits, with room left for the kernel's static shared memory.
+long long batch_group_bytes(int maxE, int maxN, int maxk, int gsize);
+constexpr long long BATCH_GROUP_BYTES_MAX = 226 * 1024;
+
+// ---- host planning helpers (delta_nabla.cpp) ------------------------------------
+long long binom_h(int n, int k);
+long long perm_h(int n, int k);
+// Common-neighbour pairs of every edge by the reference's merge walk
+// (libdress/src/dress.c:307-363): pairs[2t], pairs[2t+1] are the (u,x) and
+// (v,x) edge ids of pair t, ioff[e]..ioff[e+1] the pairs of edge e.  Also the
+// largest row and whether any row repeats a neighbour.
+void merge_walk_pairs(p_dress_graph_t g, std::vector<int> &ioff, std::vector<int> &pairs, int &maxdeg, bool &dup);
 
 }  // namespace dress

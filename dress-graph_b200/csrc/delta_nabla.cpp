@@ -27,7 +27,6 @@
 #include "hist.h"
 
 namespace dress {
-namespace {
 
 long long binom_h(int n, int k)
 {
@@ -46,6 +45,33 @@ long long perm_h(int n, int k)
     for (int i = 0; i < k; ++i) r *= (n - i);
     return r;
 }
+
+void merge_walk_pairs(p_dress_graph_t g, std::vector<int> &ioff, std::vector<int> &pairs, int &maxdeg, bool &dup)
+{
+    const int N = g->N, E = g->E;
+    const int *off = g->adj_offset, *tg = g->adj_target, *ei = g->adj_edge_idx;
+    maxdeg = 0;
+    dup = false;
+    for (int u = 0; u < N; ++u) {
+        maxdeg = std::max(maxdeg, off[u + 1] - off[u]);
+        for (int s = off[u] + 1; s < off[u + 1]; ++s) dup |= tg[s] == tg[s - 1];
+    }
+    ioff.assign((size_t)E + 1, 0);
+    pairs.clear();
+    for (int e = 0; e < E; ++e) {
+        int iu = off[g->U[e]], iu_end = off[g->U[e] + 1];
+        int iv = off[g->V[e]], iv_end = off[g->V[e] + 1];
+        while (iu < iu_end && iv < iv_end) {
+            int x = tg[iu], y = tg[iv];
+            if (x == y) { pairs.push_back(ei[iu]); pairs.push_back(ei[iv]); }
+            iu += (x <= y);
+            iv += (x >= y);
+        }
+        ioff[(size_t)e + 1] = (int)(pairs.size() / 2);
+    }
+}
+
+namespace {
 
 int lcg15(unsigned int *s)
 {
@@ -147,30 +173,16 @@ Status prepare(Prep &p)
 
     // common-neighbour pairs of the parent by the reference's merge walk
     // (libdress/src/dress.c:307-363); masks filter them per subgraph
-    const int *off = g->adj_offset, *tg = g->adj_target, *ei = g->adj_edge_idx;
     int maxdeg = 0;
     bool dup = false;
-    for (int u = 0; u < p.N; ++u) {
-        maxdeg = std::max(maxdeg, off[u + 1] - off[u]);
-        for (int s = off[u] + 1; s < off[u + 1]; ++s) dup |= tg[s] == tg[s - 1];
-    }
-    p.ioff.assign((size_t)p.E + 1, 0);
-    for (int e = 0; e < p.E; ++e) {
-        int iu = off[g->U[e]], iu_end = off[g->U[e] + 1];
-        int iv = off[g->V[e]], iv_end = off[g->V[e] + 1];
-        while (iu < iu_end && iv < iv_end) {
-            int x = tg[iu], y = tg[iv];
-            if (x == y) { p.pairs.push_back(ei[iu]); p.pairs.push_back(ei[iv]); }
-            iu += (x <= y);
-            iv += (x >= y);
-        }
-        p.ioff[(size_t)e + 1] = (int)(p.pairs.size() / 2);
-    }
+    merge_walk_pairs(g, p.ioff, p.pairs, maxdeg, dup);
     p.T = p.ioff[(size_t)p.E];
     p.M = std::max(2, next_pow2(maxdeg + 1));
     // Masks reproduce the rebuilt subgraph except for the reciprocal-weight
     // lookup of DIRECTED graphs with repeated directed edges.
-    p.batchable = p.M <= 32 && !(dup && g->variant == DRESS_VARIANT_DIRECTED);
+    // The batch kernel also needs one subgraph's state in shared memory.
+    p.batchable = p.M <= 32 && !(dup && g->variant == DRESS_VARIANT_DIRECTED) &&
+                  batch_group_bytes(p.E, p.N, k, 32) <= BATCH_GROUP_BYTES_MAX;
     return Status::Ok();
 }
 
@@ -591,7 +603,7 @@ Status finish(Prep &p)
 }  // namespace
 
 // All requests on one execution context (no locking: the caller owns ctx).
-Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const Ctx &ctx)
+Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const Ctx &ctx, int64_t *edge_sweeps)
 {
     DRESS_CUDA_TRY(cudaSetDevice(ctx.device));
     std::vector<Prep> ps((size_t)n);
@@ -659,6 +671,8 @@ Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const C
         }
         if (p.ms_host) { std::free(p.ms_host); p.ms_host = nullptr; }
     }
+    if (edge_sweeps)
+        for (int i = 0; i < n; ++i) edge_sweeps[i] = (int64_t)ps[(size_t)i].edge_iters;
     return first;
 }
 

@@ -48,13 +48,15 @@ Status Pinned::reserve(size_t bytes)
     return Status::Ok();
 }
 
-Status Ctx::create(int dev, int sms, const dressx_config_t *config)
+thread_local cudaMemPool_t tls_pool = nullptr;
+
+Status Ctx::create(int dev, int sms, const dressx_config_t *config, int priority)
 {
     device = dev;
     num_sms = sms;
     cfg = config;
-    DRESS_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    DRESS_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority));
+    DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, priority));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
     return Status::Ok();

@@ -37,10 +37,14 @@ struct Status {
     } while (0)
 
 // ---- stream-ordered device buffers -------------------------------------
-// Device memory comes from the device's default memory pool through
-// cudaMallocAsync on the engine stream.  The pool keeps freed blocks
-// (release threshold = the configured budget), so repeated calls of the same
-// size allocate nothing from the driver after the first one.
+// Device memory comes from a stream-ordered memory pool: the device's
+// default pool (release threshold = the configured budget), or, on threads
+// that set tls_pool, that pool -- a request server points its worker threads
+// at its own arena pool, so every buffer of a served request is drawn from
+// the server's resident memory.  Freed blocks stay in the pool, so repeated
+// work of the same size allocates nothing from the driver after the first.
+extern thread_local cudaMemPool_t tls_pool;
+
 template <class T>
 class DevBuf {
   public:
@@ -54,7 +58,8 @@ class DevBuf {
         st_ = st;
         n_ = n;
         if (n == 0) return Status::Ok();
-        cudaError_t e = cudaMallocAsync((void **)&p_, n * sizeof(T), st);
+        cudaError_t e = tls_pool ? cudaMallocFromPoolAsync((void **)&p_, n * sizeof(T), tls_pool, st)
+                                 : cudaMallocAsync((void **)&p_, n * sizeof(T), st);
         if (e != cudaSuccess) {
             p_ = nullptr;
             cudaGetLastError();
@@ -98,7 +103,9 @@ struct Ctx {
     cudaStream_t side = nullptr;           // concurrent hub work of the single-graph fit
     cudaEvent_t fork = nullptr, join = nullptr;
     const dressx_config_t *cfg = nullptr;
-    Status create(int dev, int sms, const dressx_config_t *config);
+    // priority: CUDA stream priority of both streams (0 = default; lower
+    // numbers are served first by the block scheduler)
+    Status create(int dev, int sms, const dressx_config_t *config, int priority = 0);
     void destroy();
 };
 
@@ -147,6 +154,9 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon,
                  int *iterations, double *delta, FitStats *stats, const Ctx &ctx);
 
 // ---- Delta/Nabla requests (delta_nabla.cpp) ---------------------------------
-Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const Ctx &ctx);
+// edge_sweeps (nullable, n entries): live edges x sweeps summed over each
+// request's fits.
+Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const Ctx &ctx,
+                       int64_t *edge_sweeps = nullptr);
 
 }  // namespace dress

@@ -353,3 +353,112 @@ def counters(reset=False):
     h, d, l = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
     lib().dressx_counters(ctypes.byref(h), ctypes.byref(d), ctypes.byref(l), 1 if reset else 0)
     return dict(h2d_bytes=h.value, d2h_bytes=d.value, launches=l.value)
+
+
+FIT = 2                                   # DRESSX_FIT (DELTA = 0, NABLA = 1)
+PATH_NONE, PATH_BATCH, PATH_LANE = 0, 1, 2
+
+
+def estimate(g: Graph, kind=FIT, k=0):
+    """Host-only plan of a served request: (device bytes reserved, path)."""
+    b, p = ctypes.c_int64(), ctypes.c_int()
+    _check(lib().dressx_server_estimate(g.ptr, int(kind), int(k), ctypes.byref(b), ctypes.byref(p)))
+    return b.value, p.value
+
+
+class Ticket:
+    """One request in a Server; ``wait()`` returns its result dict."""
+
+    def __init__(self, server, graph, kind, k, max_iterations, epsilon):
+        self.server = server
+        self.graph = graph                     # kept alive until done
+        self.req = _abi.ServerRequest()
+        r = self.req
+        r.graph = graph.ptr
+        r.kind, r.k = int(kind), int(k)
+        r.max_iterations, r.epsilon = int(max_iterations), float(epsilon)
+        self.code = lib().dressx_server_submit(server.handle, ctypes.byref(r))
+        self._result = None
+
+    @property
+    def done(self):
+        return bool(self.req.done)
+
+    def wait(self, timeout_ms=-1):
+        code = lib().dressx_server_wait(self.server.handle, ctypes.byref(self.req), int(timeout_ms))
+        if code == 4 and not self.req.done:            # DRESSX_ETIMEOUT
+            raise TimeoutError("request still in service")
+        return self.result()
+
+    def cancel(self):
+        return lib().dressx_server_cancel(self.server.handle, ctypes.byref(self.req))
+
+    def result(self):
+        if self._result is not None:
+            return self._result
+        r = self.req
+        if not r.done:
+            return None
+        out = dict(status=r.status, path=r.path, queue_ms=r.queue_ms, latency_ms=r.latency_ms,
+                   reserved_bytes=r.reserved_bytes, fits=r.fits, edge_sweeps=r.edge_sweeps)
+        if r.kind == FIT:
+            out.update(iterations=r.iterations, delta=r.delta)
+        else:
+            flat = _arr(r.hist_flat, r.hist_len, np.int64)
+            if r.hist_flat:
+                lib().dressx_free(ctypes.cast(r.hist_flat, ctypes.c_void_p))
+                r.hist_flat = None
+            out.update(hist_flat=flat, num_subgraphs=r.num_subgraphs)
+        self._result = out
+        return out
+
+
+class Server:
+    """A continuous-batching request server (``dressx_server_*``): submit
+    fits and Delta/Nabla requests from any thread; small ones share short
+    persistent batch launches, large ones run on lanes beside them, all
+    admitted against a device-memory budget."""
+
+    def __init__(self, memory_budget_bytes=0, lanes=0, launch_slots=0, launch_work=0, finishers=0,
+                 max_queued=0, device=-1):
+        cfg = _abi.ServerConfig()
+        cfg.device = int(device)
+        cfg.memory_budget_bytes = int(memory_budget_bytes)
+        cfg.lanes, cfg.launch_slots = int(lanes), int(launch_slots)
+        cfg.launch_work, cfg.finishers = int(launch_work), int(finishers)
+        cfg.max_queued = int(max_queued)
+        h = ctypes.c_void_p()
+        _check(lib().dressx_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self.handle = h
+
+    def submit(self, graph: Graph, kind=FIT, k=0, max_iterations=100, epsilon=1e-6) -> Ticket:
+        return Ticket(self, graph, kind, k, max_iterations, epsilon)
+
+    def drain(self, timeout_ms=-1):
+        _check(lib().dressx_server_drain(self.handle, int(timeout_ms)))
+
+    def stats(self, reset=False):
+        st = _abi.ServerStats()
+        _check(lib().dressx_server_stats(self.handle, ctypes.byref(st), 1 if reset else 0))
+        out = {name: getattr(st, name) for name, _ in _abi.ServerStats._fields_ if name != "cls"}
+        for i, name in enumerate(_abi.SERVER_CLASSES):
+            c = st.cls[i]
+            out[name] = {f: getattr(c, f) for f, _ in _abi.ServerClassStats._fields_}
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().dressx_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -62,6 +62,54 @@ class FitStats(ctypes.Structure):
                 ("setup_ms", ctypes.c_double), ("iterate_ms", ctypes.c_double)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int), ("memory_budget_bytes", ctypes.c_size_t),
+        ("lanes", ctypes.c_int), ("launch_slots", ctypes.c_int),
+        ("launch_work", ctypes.c_int64), ("finishers", ctypes.c_int),
+        ("max_queued", ctypes.c_int), ("reserved", ctypes.c_int * 8),
+    ]
+
+
+class ServerRequest(ctypes.Structure):
+    _fields_ = [
+        ("graph", PGraph), ("kind", ctypes.c_int), ("k", ctypes.c_int),
+        ("max_iterations", ctypes.c_int), ("epsilon", ctypes.c_double),
+        ("iterations", ctypes.c_int), ("delta", ctypes.c_double),
+        ("hist_flat", _c_i64_p), ("hist_len", ctypes.c_int),
+        ("num_subgraphs", ctypes.c_int64), ("fits", ctypes.c_int64),
+        ("edge_sweeps", ctypes.c_int64), ("path", ctypes.c_int), ("status", ctypes.c_int),
+        ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+        ("reserved_bytes", ctypes.c_int64), ("done", ctypes.c_int),
+    ]
+
+
+class ServerClassStats(ctypes.Structure):
+    _fields_ = [
+        ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+        ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+        ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+        ("queue_p50_ms", ctypes.c_double), ("queue_p99_ms", ctypes.c_double),
+    ]
+
+
+SERVER_CLASSES = ("fit_batch", "fit_lane", "hist_batch", "hist_lane")
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("elapsed_s", ctypes.c_double),
+        ("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+        ("cancelled", ctypes.c_int64), ("rejected", ctypes.c_int64),
+        ("fits", ctypes.c_int64), ("edge_sweeps", ctypes.c_int64), ("batch_launches", ctypes.c_int64),
+        ("budget_bytes", ctypes.c_int64), ("reserved_bytes", ctypes.c_int64),
+        ("peak_reserved_bytes", ctypes.c_int64), ("pool_bytes", ctypes.c_int64),
+        ("max_in_service", ctypes.c_int),
+        ("device_busy_ms", ctypes.c_double), ("device_work_ms", ctypes.c_double),
+        ("cls", ServerClassStats * 4),
+    ]
+
+
 _HIST_ARGS = [PGraph, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
               ctypes.c_uint, _c_int_p, ctypes.c_int, ctypes.POINTER(_c_dbl_p), _c_i64_p]
 
@@ -95,6 +143,14 @@ SIGNATURES = {
     "dressx_batch_destroy": (None, [ctypes.c_void_p]),
     "dressx_stream": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p)]),
     "dressx_counters": (ctypes.c_int, [_c_i64_p, _c_i64_p, _c_i64_p, ctypes.c_int]),
+    "dressx_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "dressx_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerRequest)]),
+    "dressx_server_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerRequest), ctypes.c_int]),
+    "dressx_server_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerRequest)]),
+    "dressx_server_drain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "dressx_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats), ctypes.c_int]),
+    "dressx_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "dressx_server_estimate": (ctypes.c_int, [PGraph, ctypes.c_int, ctypes.c_int, _c_i64_p, _c_int_p]),
     "dressx_histogram_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                                                 ctypes.c_void_p]),
 }

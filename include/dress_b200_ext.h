@@ -148,6 +148,122 @@ int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, i
 int dressx_histogram_noalloc(const double *values, int64_t n, int64_t *pairs, int64_t *num_runs,
                              void *stream);
 
+/* ---- Request server ----------------------------------------------------
+ * No counterpart in the reference: its CUDA backend fits one graph per call
+ * on the legacy stream.  A server takes fit and Delta/Nabla requests from
+ * any number of host threads as they arrive and serves them concurrently:
+ *   - admission: a request reserves an estimate of its device memory from
+ *     the server's budget; requests wait in arrival order until it fits
+ *     (one larger than the whole budget fails with DRESSX_EBUDGET);
+ *   - residency: admitted requests keep their packed graph and edge state in
+ *     the server's own memory pool (an arena that keeps its memory between
+ *     requests) until they complete;
+ *   - continuous batching: small requests (every row of at most 31
+ *     neighbours, state within shared memory) are cut into slices and packed
+ *     into short persistent batch launches, a few in flight at once; a
+ *     request that arrives while launches run joins the next launch, every
+ *     waiting request gets a share of each launch, and a request completes as
+ *     soon as its last slice has run;
+ *   - lanes: larger requests run on their own streams (the single-graph fit,
+ *     or the per-subgraph Delta/Nabla path), beside the batch launches;
+ *   - latency: each request records its queueing and end-to-end time; the
+ *     statistics give p50/p99 per class.
+ * Results are bit-identical to the single-request calls (dressx_fit,
+ * dressx_hist_batch), whatever else is in service. */
+typedef struct dressx_server dressx_server_t;
+
+typedef struct dressx_server_config_t {
+    int     device;               /* CUDA device ordinal; -1 = current        */
+    size_t  memory_budget_bytes;  /* admission budget; 0 = 120 GiB, at most
+                                     90% of the device memory free at create */
+    int     lanes;                /* concurrent large requests; 0 = 2          */
+    int     launch_slots;         /* batch launches in flight; 0 = 3           */
+    int64_t launch_work;          /* edge-subgraph units per batch launch
+                                     (sum of edges over its fits); 0 = 2^21   */
+    int     finishers;            /* threads building results; 0 = 2           */
+    int     max_queued;           /* requests waiting for admission; 0 = 65536 */
+    int     reserved[8];
+} dressx_server_config_t;
+
+/* Request kinds: DRESSX_DELTA, DRESSX_NABLA (above) and a plain fit. */
+enum { DRESSX_FIT = 2 };
+
+/* Where a request was served. */
+enum { DRESSX_PATH_NONE = 0, DRESSX_PATH_BATCH = 1, DRESSX_PATH_LANE = 2 };
+
+/* Statistics classes: kind x path. */
+enum { DRESSX_CLASS_FIT_BATCH = 0, DRESSX_CLASS_FIT_LANE = 1,
+       DRESSX_CLASS_HIST_BATCH = 2, DRESSX_CLASS_HIST_LANE = 3, DRESSX_CLASSES = 4 };
+
+typedef struct dressx_server_request_t {
+    /* inputs; the graph must stay alive and unchanged until `done` */
+    p_dress_graph_t graph;
+    int      kind;               /* DRESSX_FIT, DRESSX_DELTA, DRESSX_NABLA   */
+    int      k;                  /* Delta/Nabla order                        */
+    int      max_iterations;
+    double   epsilon;
+    /* outputs.  DRESSX_FIT updates graph->edge_dress and vertex_dress in
+     * place, as dress_fit does, and sets iterations / delta (delta is left
+     * as it was when max_iterations <= 0).  Delta/Nabla return the exact
+     * histogram, malloc'd (free with free() or dressx_free). */
+    int      iterations;
+    double   delta;
+    int64_t *hist_flat;          /* [value_bits, count, ...] ascending       */
+    int      hist_len;           /* 2 * distinct values                      */
+    int64_t  num_subgraphs;      /* C(N,k) or P(N,k)                         */
+    int64_t  fits;               /* fits run for this request                */
+    int64_t  edge_sweeps;        /* sum over fits of live edges x sweeps     */
+    int      path;               /* DRESSX_PATH_*                            */
+    int      status;             /* DRESSX_* of this request                 */
+    double   queue_ms;           /* submission -> admission                  */
+    double   latency_ms;         /* submission -> completion                 */
+    int64_t  reserved_bytes;     /* device memory reserved at admission      */
+    volatile int done;           /* 1 once every output above is final       */
+} dressx_server_request_t;
+
+typedef struct dressx_server_class_stats_t {
+    int64_t completed, failed;
+    double  p50_ms, p99_ms, mean_ms, max_ms;     /* end-to-end latency       */
+    double  queue_p50_ms, queue_p99_ms;          /* waiting for admission    */
+} dressx_server_class_stats_t;
+
+typedef struct dressx_server_stats_t {
+    double   elapsed_s;           /* since create or the last reset          */
+    int64_t  submitted, completed, failed, cancelled, rejected;
+    int64_t  fits;                /* subgraph and graph fits completed       */
+    int64_t  edge_sweeps;         /* live edges x sweeps over those fits     */
+    int64_t  batch_launches;
+    int64_t  budget_bytes, reserved_bytes, peak_reserved_bytes;
+    int64_t  pool_bytes;          /* device memory the arena pool holds      */
+    int      max_in_service;      /* most requests admitted at once          */
+    double   device_busy_ms;      /* union of the device intervals of batch
+                                     launches and lane requests              */
+    double   device_work_ms;      /* their sum (> busy when work overlapped) */
+    dressx_server_class_stats_t cls[DRESSX_CLASSES];
+} dressx_server_stats_t;
+
+int  dressx_server_create(const dressx_server_config_t *cfg, dressx_server_t **out);
+/* Queue a request (the struct must stay alive until done).  Returns
+ * DRESSX_OK once queued; a request refused at once (bad arguments, larger
+ * than the budget, queue full) returns its status and is marked done. */
+int  dressx_server_submit(dressx_server_t *s, dressx_server_request_t *req);
+/* Wait until req is done: its status, or DRESSX_ETIMEOUT after timeout_ms
+ * (negative = no limit). */
+int  dressx_server_wait(dressx_server_t *s, dressx_server_request_t *req, int timeout_ms);
+/* Cancel a request that has not started device work (DRESSX_OK; it ends
+ * with DRESSX_ECANCELLED), or a Delta/Nabla batch request between slices;
+ * DRESSX_EBUSY when it is too late. */
+int  dressx_server_cancel(dressx_server_t *s, dressx_server_request_t *req);
+/* Wait until no request is queued or in service. */
+int  dressx_server_drain(dressx_server_t *s, int timeout_ms);
+int  dressx_server_stats(dressx_server_t *s, dressx_server_stats_t *out, int reset);
+/* Cancels queued requests, finishes admitted ones, frees the arena. */
+int  dressx_server_destroy(dressx_server_t *s);
+
+/* Host-only planning of a request (no device needed): the device memory it
+ * would reserve and the path it would take. */
+int  dressx_server_estimate(p_dress_graph_t g, int kind, int k, int64_t *bytes, int *path);
+
 /* Frees a buffer returned by this library. */
 void dressx_free(void *p);
 
