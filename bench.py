@@ -18,6 +18,13 @@ subgraph fits plus the 2,000 histograms.  Metric: subgraph-fits/s.
   (compiled from its sources into oracle/_ref) on a bounded sample.
 * ``single_fit``: the 28M-edge Chung-Lu fit (BASELINE config "single large
   fit"), edge-iters/s and the HBM roofline of its sweeps.
+* ``serving``: a stream of fit and Delta^1 requests (BASELINE config
+  "serving stream") submitted to the request server at Poisson arrival rates
+  swept over ``--serve-rates``: graphs/s, subgraph-fits/s, p50/p99 latency
+  per request kind and per path, device overlap, admission statistics, a
+  spot check that served results equal the same requests run alone, and the
+  reference's sequential single-thread calls on the same stream as the CPU
+  baseline.
 
 ``--impl reference`` times the reference's own CPU implementation
 (``dress_delta_fit_omp``, all host threads) on a bounded sample of the same
@@ -55,6 +62,9 @@ def parse():
     ap.add_argument("--no-single-fit", action="store_true", help="skip the 28M-edge single fit")
     ap.add_argument("--single-fit-edges", type=int, default=28_000_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving stream")
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-rates", default="20,80,320", help="Poisson arrival rates (requests/s) to sweep")
     return ap.parse_args()
 
 
@@ -321,6 +331,126 @@ def bench_single_fit(args, torch):
 
 
 # ---------------------------------------------------------------------------
+# serving: Poisson arrivals of fit and Delta^1 requests through the server
+# ---------------------------------------------------------------------------
+
+def _reset_edges(g):
+    """Edge values back to the initial 1.0 (a fit continues from them)."""
+    if g.E:
+        np.ctypeslib.as_array(g.ptr.contents.edge_dress, shape=(g.E,))[:] = 1.0
+
+
+def _pct(v, q):
+    if not v:
+        return None
+    v = sorted(v)
+    return v[max(0, int(np.ceil(q * len(v))) - 1)]
+
+
+def bench_serving(args, clocks):
+    import dress_b200 as db
+    from dress_b200 import graphs
+    reqs = graphs.serving_stream(args.serve_requests, seed=5)
+    objs = [db.Graph(n, U, V, W) for (_, n, U, V, W) in reqs]
+    kinds = [k for k, *_ in reqs]
+    names = {0: "delta1", 2: "fit"}
+    out = {"workload": f"{len(reqs)} requests: {sum(k == 0 for k in kinds)} Delta^1 (edges log-uniform 10..5K) and "
+                       f"{sum(k == 2 for k in kinds)} fits (edges log-uniform 10..1M); random d-regular below 5K "
+                       "edges, Chung-Lu (gamma 2.3, mean degree 14) above; 30% weighted U[0.5,2]; epsilon 1e-6",
+           "total_edges": int(sum(g.E for g in objs)), "rates": []}
+    clocks.start()
+    with db.Server() as srv:
+        # warm-up pass over the first requests (kernel attributes, arena growth)
+        for g in objs[:20]:
+            _reset_edges(g)
+        ws = [srv.submit(g, k, 1 if k == 0 else 0) for g, k in zip(objs[:20], kinds[:20])]
+        srv.drain()
+        assert all(t.result()["status"] == 0 for t in ws)
+        for rate in [float(x) for x in args.serve_rates.split(",") if x]:
+            for g in objs:
+                _reset_edges(g)
+            gaps = np.random.default_rng(17).exponential(1.0 / rate, len(objs))
+            srv.stats(reset=True)
+            db.counters(reset=True)
+            tickets = []
+            t0 = time.perf_counter()
+            due = t0
+            for g, k, gap in zip(objs, kinds, gaps):
+                due += gap
+                wait = due - time.perf_counter()
+                if wait > 0:
+                    time.sleep(wait)
+                tickets.append(srv.submit(g, k, 1 if k == 0 else 0))
+            srv.drain()
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+            cnt = db.counters()
+            res = [t.result() for t in tickets]
+            lat = {name: [r["latency_ms"] for r, k in zip(res, kinds) if k == kk] for kk, name in names.items()}
+            allv = [r["latency_ms"] for r in res]
+            row = {
+                "offered_rate": rate, "wall_s": wall, "completed": st["completed"], "failed": st["failed"],
+                "graphs_per_s": st["completed"] / wall, "subgraph_fits_per_s": st["fits"] / wall,
+                "edge_sweeps_per_s": st["edge_sweeps"] / wall,
+                "p50_ms": _pct(allv, 0.5), "p99_ms": _pct(allv, 0.99),
+                "by_kind": {name: {"n": len(v), "p50_ms": _pct(v, 0.5), "p99_ms": _pct(v, 0.99)}
+                            for name, v in lat.items()},
+                "by_path": {name: {"n": st[name]["completed"], "p50_ms": st[name]["p50_ms"],
+                                   "p99_ms": st[name]["p99_ms"], "queue_p99_ms": st[name]["queue_p99_ms"]}
+                            for name in ("fit_batch", "fit_lane", "hist_batch", "hist_lane")},
+                "batch_launches": st["batch_launches"], "gpu_launches": cnt["launches"],
+                "device_busy_ms": st["device_busy_ms"], "device_work_ms": st["device_work_ms"],
+                "overlap": st["device_work_ms"] / st["device_busy_ms"] if st["device_busy_ms"] else None,
+                "max_in_service": st["max_in_service"], "peak_reserved_bytes": st["peak_reserved_bytes"],
+                "pool_bytes": st["pool_bytes"], "budget_bytes": st["budget_bytes"],
+                "h2d_bytes": cnt["h2d_bytes"], "d2h_bytes": cnt["d2h_bytes"],
+            }
+            out["rates"].append(row)
+        # spot check: served results equal the same requests run alone
+        rng = np.random.default_rng(3)
+        idx = rng.choice(len(objs), size=min(12, len(objs)), replace=False)
+        served_fit = {int(i): objs[int(i)].edge_dress for i in idx if kinds[int(i)] == 2}
+        same = True
+        for i in idx:
+            i = int(i)
+            if kinds[i] == 0:
+                flat = db.hist_requests([objs[i]], db.DELTA, 1)[0][0]
+                same &= bool(np.array_equal(flat, tickets[i].result()["hist_flat"]))
+            else:
+                _reset_edges(objs[i])
+                db.fit_graph(objs[i], 100, 1e-6)
+                same &= bool(np.array_equal(objs[i].edge_dress.view(np.int64), served_fit[i].view(np.int64)))
+        out["same_alone_and_in_mix"] = {"checked": len(idx), "identical": same}
+    out["clocks"] = clocks.stop()
+
+    # CPU: the reference's sequential single-thread calls, requests in arrival order
+    import oracle
+    cpu = oracle.reference()
+    kind = "reference" if cpu is not None else "port"
+    cpu = cpu or oracle.port()
+    t0 = time.perf_counter()
+    done, per = 0, {"fit": [], "delta1": []}
+    for (k, n, U, V, W) in reqs:
+        t1 = time.perf_counter()
+        if k == 0:
+            cpu.delta_fit(n, U, V, W, k=1)
+        else:
+            cpu.fit(n, U, V, W)
+        per[names[k]].append((time.perf_counter() - t1) * 1e3)
+        done += 1
+        if time.perf_counter() - t0 > args.cpu_seconds:
+            break
+    dt = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": done / dt, "unit": "requests/s", "cores": 1, "kind": kind,
+                           "sample": f"first {done} requests of the stream in arrival order, one at a time "
+                                     f"({dt:.1f} s)",
+                           "mean_ms": {kk: (sum(v) / len(v) if v else None) for kk, v in per.items()}}
+    for g in objs:
+        g.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # the reference arm: the reference's own CPU implementation
 # ---------------------------------------------------------------------------
 
@@ -382,6 +512,7 @@ def main():
     clocks = Clocks(local)
     head = bench_delta1(args, rank, world, pg, torch, clocks)
     single = None
+    serving = None
     cpu = None
     if rank == 0 and world == 1:
         v, used, fits, dt = cpu_delta1_sample(head["gs"], args.cpu_seconds,
@@ -391,6 +522,8 @@ def main():
                "sample": f"single-thread dress_delta_fit on the first {used} graphs ({fits} fits, {dt:.1f} s)"}
         if not args.no_single_fit:
             single = bench_single_fit(args, torch)
+        if not args.no_serving:
+            serving = bench_serving(args, Clocks(local))
     if rank == 0:
         clk = head["clocks"]
         line = {
@@ -407,7 +540,7 @@ def main():
             "e2e": head["e2e"], "gpu_launches": head["launches"], "roofline": head["roofline"],
             "cpu_baseline": cpu, "per_fit_gpu": head["per_fit"],
             "breakdown_ms": {"fits": head["fit_ms"], "histograms": head["hist_ms"], "wall": head["wall_ms"]},
-            "clocks": clk, "single_fit": single,
+            "clocks": clk, "single_fit": single, "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

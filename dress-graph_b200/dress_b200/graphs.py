@@ -142,3 +142,32 @@ def regular_batch(count, n_range=(16, 100), d_range=(3, 12), seed=42):
 
 def uniform_weights(m, lo=0.5, hi=2.0, seed=7):
     return np.random.default_rng(seed).uniform(lo, hi, m)
+
+
+def serving_stream(count, seed=5, fit_edges=(10, 1_000_000), delta_edges=(10, 5000), delta_frac=0.3,
+                   weighted_frac=0.3, regular_below=5000):
+    """Requests of a serving workload: ``count`` tuples (kind, n, U, V, W)
+    with kind 2 (fit) or 0 (Delta^1) (a ``delta_frac`` share), edge counts
+    log-uniform in ``fit_edges`` / ``delta_edges``, random d-regular graphs
+    (d ~ U{3..12}) below ``regular_below`` edges and Chung-Lu power-law
+    graphs (mean degree 14, gamma 2.3) above, a ``weighted_frac`` share with
+    U[0.5, 2.0] edge weights."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        kind = 0 if rng.random() < delta_frac else 2
+        lo, hi = delta_edges if kind == 0 else fit_edges
+        m = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        s = int(rng.integers(1 << 31))
+        if m < regular_below:
+            d = int(rng.integers(3, 13))
+            n = max(d + 1, (2 * m) // d)
+            if (n * d) % 2:
+                n += 1
+            n, U, V = random_regular(n, d, seed=s)
+        else:
+            n = max(16, m // 7)
+            n, U, V = chung_lu(n, m, 2.3, min(20000, n // 2), seed=s)
+        W = uniform_weights(len(U), seed=s + 1) if rng.random() < weighted_frac else None
+        out.append((kind, n, U, V, W))
+    return out
