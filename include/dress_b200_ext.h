@@ -148,6 +148,15 @@ int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, i
 int dressx_histogram_noalloc(const double *values, int64_t n, int64_t *pairs, int64_t *num_runs,
                              void *stream);
 
+/* Merge of histograms computed on disjoint shards of one request (e.g. the
+ * strided slices offset = rank, stride = ranks of several GPUs or
+ * processes): n flat [value_bits, count, ...] lists, each ascending by value,
+ * into one list of the same form (malloc'd; *out_len entries).  Counts of
+ * ==-equal values add up.  Replaces the gather-and-reinsert step of the
+ * reference's MPI layer (libdress/src/mpi/dress_mpi.c:90-118). */
+int dressx_hist_merge(const int64_t *const *flats, const int64_t *lens, int n, int64_t **out,
+                      int64_t *out_len);
+
 /* ---- Request server ----------------------------------------------------
  * No counterpart in the reference: its CUDA backend fits one graph per call
  * on the legacy stream.  A server takes fit and Delta/Nabla requests from
