@@ -18,6 +18,10 @@ subgraph fits plus the 2,000 histograms.  Metric: subgraph-fits/s.
   (compiled from its sources into oracle/_ref) on a bounded sample.
 * ``single_fit``: the 28M-edge Chung-Lu fit (BASELINE config "single large
   fit"), edge-iters/s and the HBM roofline of its sweeps.
+* ``delta2_nabla1``: Delta^2 and Nabla^1 of 64 random 10-regular graphs of
+  200 vertices, autotuned and replayed from a CUDA graph.
+* ``plain_fit``: one G(2000, 10000) fit through
+  dress_fit_cuda and through the server's batch path.
 * ``serving``: a stream of fit and Delta^1 requests (BASELINE config
   "serving stream") submitted to the request server at Poisson arrival rates
   swept over ``--serve-rates``: graphs/s, subgraph-fits/s, p50/p99 latency
@@ -63,6 +67,8 @@ def parse():
     ap.add_argument("--single-fit-edges", type=int, default=28_000_000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving stream")
+    ap.add_argument("--no-k2", action="store_true", help="skip the Delta^2 / Nabla^1 workload")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-fit workload")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-rates", default="20,80,320", help="Poisson arrival rates (requests/s) to sweep")
     return ap.parse_args()
@@ -331,6 +337,148 @@ def bench_single_fit(args, torch):
 
 
 # ---------------------------------------------------------------------------
+# Delta^2 and Nabla^1 on 64 random 10-regular graphs of 200 vertices
+# ---------------------------------------------------------------------------
+
+def bench_k2(args, clocks):
+    import dress_b200 as db
+    from dress_b200 import graphs
+    gs = [graphs.random_regular(200, 10, seed=1000 + i) for i in range(64)]
+    objs = [db.Graph(n, U, V) for n, U, V in gs]
+    out = {"workload": "64 random 10-regular graphs, n=200 (1,000 edges each), epsilon 1e-6; Delta^2 "
+                       "(C(200,2)=19,900 subgraphs per graph) and Nabla^1 (200 marked fits per graph); "
+                       "autotuned threads per subgraph, fit stage replayed from a CUDA graph",
+           "l2": "values of a step (10 GB for Delta^2) exceed L2; parents are staged in shared memory"}
+    clocks.start()
+    for label, kind, k in (("delta2", db.DELTA, 2), ("nabla1", db.NABLA, 1)):
+        b = db.Batch(objs, kind, k)
+        t0 = time.perf_counter()
+        best, rates = b.autotune()
+        tune_s = time.perf_counter() - t0
+        b.capture()
+        b.run()                                  # warm-up
+        steps = min(args.steps, 3) if label == "delta2" else args.steps
+        fit_ms = hist_ms = 0.0
+        db.counters(reset=True)
+        for _ in range(steps):
+            b.run()
+            f, h = b.timing()
+            fit_ms += f
+            hist_ms += h
+        launches = db.counters()["launches"]
+        st = b.stats()
+        step_ms = (fit_ms + hist_ms) / steps
+        out[label] = {
+            "value": st["fits"] / (step_ms / 1e3), "unit": "subgraph-fits/s", "steps": steps,
+            "fits_per_step": st["fits"], "edge_updates_per_step": st["edge_updates"],
+            "edge_sweeps_per_s": st["edge_updates"] / (fit_ms / steps / 1e3),
+            "fit_ms": fit_ms / steps, "hist_ms": hist_ms / steps, "ms_per_step": step_ms,
+            "gpu_launches_per_step": launches / steps,
+            "autotune": {"threads_per_subgraph": best, "sampled_fits_per_ms": rates, "seconds": tune_s},
+            "cuda_graph": True,
+        }
+        b.close()
+    out["clocks"] = clocks.stop()
+    # end to end through the C ABI on a sample of 4 graphs (a full step's
+    # histograms are ~20 GB of host memory)
+    t0 = time.perf_counter()
+    res = db.hist_requests(objs[:4], db.DELTA, 2)
+    dt = time.perf_counter() - t0
+    out["delta2"]["e2e_sample"] = {"value": sum(r[3] for r in res) / dt, "unit": "subgraph-fits/s",
+                                   "sample": "first 4 of the 64 graphs, one dressx_hist_batch call",
+                                   "distinct_values": int(sum(r[0].size // 2 for r in res))}
+    # CPU: the reference's single-thread strided call on graph 0, extrapolated
+    import oracle
+    cpu = oracle.reference()
+    kind = "reference" if cpu is not None else "port"
+    cpu = cpu or oracle.port()
+    n, U, V = gs[0]
+    for label, fn, k, stride, per_graph in (("delta2", cpu.delta_fit, 2, 199, 19900),
+                                            ("nabla1", cpu.nabla_fit, 1, 10, 200)):
+        t0 = time.perf_counter()
+        fn(n, U, V, k=k, offset=0, stride=stride)
+        dt = time.perf_counter() - t0
+        fits = -(-per_graph // stride)
+        out[label]["cpu_baseline"] = {
+            "value": fits / dt, "unit": "subgraph-fits/s", "cores": 1, "kind": kind,
+            "sample": f"graph 0, strided slice offset 0 stride {stride} ({fits} fits, {dt:.2f} s); "
+                      f"extrapolated step time {64 * per_graph / (fits / dt):.0f} s"}
+    for g in objs:
+        g.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# plain fit: one Erdos-Renyi graph, n=2000, m=10000
+# ---------------------------------------------------------------------------
+
+def bench_plain(args):
+    import dress_b200 as db
+    from dress_b200 import graphs
+    n, U, V = graphs.erdos_renyi(2000, 10000, seed=42)
+    E = len(U)
+    out = {"workload": "Erdos-Renyi G(2000, 10000), seed 42, unweighted, undirected, epsilon 1e-6, max 100"}
+    g = db.Graph(n, U, V)
+    for _ in range(3):
+        _reset_edges(g)
+        db.fit_graph(g, 100, 1e-6)
+    reps = 20
+    t0 = time.perf_counter()
+    dev = 0.0
+    for _ in range(reps):
+        _reset_edges(g)
+        it, dl = db.fit_graph(g, 100, 1e-6)
+        st = db.last_fit_stats()
+        dev += st["iterate_ms"] + st["setup_ms"]
+    wall = time.perf_counter() - t0
+    sweeps = st["sweeps"]
+    out["dress_fit_cuda"] = {"fits_per_s": reps / wall, "ms_per_fit": wall * 1e3 / reps,
+                             "device_ms_per_fit": dev / reps, "iterations": it, "sweeps": sweeps,
+                             "edge_iters_per_s": E * sweeps * reps / wall}
+    # the same fit through the server's batch path (one request at a time, and 64 in flight)
+    with db.Server() as srv:
+        for _ in range(3):
+            _reset_edges(g)
+            srv.submit(g, db.FIT).wait()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            _reset_edges(g)
+            r = srv.submit(g, db.FIT).wait()
+        wall1 = time.perf_counter() - t0
+        many = [db.Graph(n, U, V) for _ in range(64)]
+        t0 = time.perf_counter()
+        ts = [srv.submit(x, db.FIT) for x in many]
+        for t in ts:
+            t.wait()
+        wall64 = time.perf_counter() - t0
+        same = all(np.array_equal(x.edge_dress.view(np.int64), g.edge_dress.view(np.int64)) for x in many)
+        for x in many:
+            x.close()
+    out["served"] = {"path": r["path"], "ms_per_fit_alone": wall1 * 1e3 / reps,
+                     "fits_per_s_64_in_flight": 64 / wall64, "identical_to_dress_fit_cuda": bool(same)}
+    g.close()
+    import oracle
+    cpu = oracle.reference()
+    kind = "reference" if cpu is not None else "port"
+    cpu = cpu or oracle.port()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        cpu.fit(n, U, V)
+    dt1 = (time.perf_counter() - t0) / 3
+    res = {"single_thread": {"value": 1.0 / dt1, "unit": "fits/s", "cores": 1, "kind": kind,
+                             "sample": "3 fits, dress_fit"}}
+    if kind == "reference":
+        t0 = time.perf_counter()
+        for _ in range(3):
+            cpu.fit(n, U, V, omp=True)
+        dto = (time.perf_counter() - t0) / 3
+        res["omp"] = {"value": 1.0 / dto, "unit": "fits/s", "cores": len(os.sched_getaffinity(0)),
+                      "kind": kind, "sample": "3 fits, dress_fit_omp"}
+    out["cpu_baseline"] = res
+    return out
+
+
+# ---------------------------------------------------------------------------
 # serving: Poisson arrivals of fit and Delta^1 requests through the server
 # ---------------------------------------------------------------------------
 
@@ -512,7 +660,7 @@ def main():
     clocks = Clocks(local)
     head = bench_delta1(args, rank, world, pg, torch, clocks)
     single = None
-    serving = None
+    serving = k2 = plain = None
     cpu = None
     if rank == 0 and world == 1:
         v, used, fits, dt = cpu_delta1_sample(head["gs"], args.cpu_seconds,
@@ -524,6 +672,10 @@ def main():
             single = bench_single_fit(args, torch)
         if not args.no_serving:
             serving = bench_serving(args, Clocks(local))
+        if not args.no_k2:
+            k2 = bench_k2(args, Clocks(local))
+        if not args.no_plain:
+            plain = bench_plain(args)
     if rank == 0:
         clk = head["clocks"]
         line = {
@@ -540,7 +692,7 @@ def main():
             "e2e": head["e2e"], "gpu_launches": head["launches"], "roofline": head["roofline"],
             "cpu_baseline": cpu, "per_fit_gpu": head["per_fit"],
             "breakdown_ms": {"fits": head["fit_ms"], "histograms": head["hist_ms"], "wall": head["wall_ms"]},
-            "clocks": clk, "single_fit": single, "serving": serving,
+            "clocks": clk, "single_fit": single, "serving": serving, "delta2_nabla1": k2, "plain_fit": plain,
         }
         print(json.dumps(line), flush=True)
     if pg is not None:

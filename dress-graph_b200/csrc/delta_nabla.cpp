@@ -18,6 +18,8 @@
 // measured against).  Histograms are always built on the GPU.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -327,16 +329,78 @@ struct Tune {
 };
 
 // Threads per subgraph by edge count (sweeps of a few hundred edges keep a
-// warp busy; larger subgraphs split across more warps).
-Tune pick_tune(int maxE, int maxN, int M, const dressx_config_t &cfg)
+// warp busy; larger subgraphs split across more warps), unless the autotuner
+// has measured this size class.
+struct TuneKey {
+    int e, n, M, k;
+    bool operator<(const TuneKey &o) const
+    {
+        return e != o.e ? e < o.e : n != o.n ? n < o.n : M != o.M ? M < o.M : k < o.k;
+    }
+};
+std::mutex g_tuned_mu;
+std::map<TuneKey, int> g_tuned;     // size class -> measured best threads per subgraph
+
+TuneKey tune_key(int maxE, int maxN, int M, int maxk)
+{
+    return {next_pow2(maxE), next_pow2(maxN), M, maxk};
+}
+
+Tune pick_tune(int maxE, int maxN, int M, int maxk, const dressx_config_t &cfg)
 {
     int gs = cfg.group_threads > 0 ? cfg.group_threads
            : maxE <= 640 ? 32 : maxE <= 2048 ? 64 : maxE <= 8192 ? 128 : 256;
-    (void)maxN;
-    (void)M;
+    if (cfg.group_threads <= 0) {
+        std::lock_guard<std::mutex> lk(g_tuned_mu);
+        auto it = g_tuned.find(tune_key(maxE, maxN, M, maxk));
+        if (it != g_tuned.end()) gs = it->second;
+    }
     int groups = 512 / gs;
     if (gs > 32 && groups > 15) groups = 15;
     return {gs, groups};
+}
+
+// Groups per CTA and parent staging for a given group size: as many groups
+// as shared memory holds (at most `groups`), staging the parent unless that
+// halves the groups.  False when not even one group fits.
+bool shape_launch(BatchLaunch &L, const Tune &tu, long long smem_cap)
+{
+    L.gsize = tu.gsize;
+    L.per_group = 0;
+    L.stage = 1;
+    L.groups = tu.groups;
+    while (L.groups > 1 && (long long)batch_smem_bytes(L) > smem_cap) --L.groups;
+    if ((long long)batch_smem_bytes(L) > smem_cap) {
+        L.stage = 0;
+        L.groups = tu.groups;
+        while (L.groups > 1 && (long long)batch_smem_bytes(L) > smem_cap) --L.groups;
+    }
+    if ((long long)batch_smem_bytes(L) > smem_cap) return false;
+    if (L.stage && L.groups * 2 < tu.groups) {
+        // staging leaves too few groups: read parents from L2 instead
+        BatchLaunch L2 = L;
+        L2.stage = 0;
+        L2.groups = tu.groups;
+        while (L2.groups > 1 && (long long)batch_smem_bytes(L2) > smem_cap) --L2.groups;
+        if (L2.groups > L.groups) L = L2;
+    }
+    return true;
+}
+
+// Chunks: a few rounds of subgraphs per CTA visit, requests in order; with
+// limit >= 0 only the first `limit` subgraphs of the whole batch.
+void build_chunks(const std::vector<Prep *> &ps, int groups, long long limit, std::vector<Chunk> &chunks)
+{
+    chunks.clear();
+    const int chunk_items = 4 * groups;
+    long long taken = 0;
+    for (size_t i = 0; i < ps.size(); ++i)
+        for (long long f = 0; f < ps[i]->items; f += chunk_items) {
+            if (limit >= 0 && taken >= limit) return;
+            int c = (int)std::min<long long>(chunk_items, ps[i]->items - f);
+            chunks.push_back({(int)i, c, f});
+            taken += c;
+        }
 }
 
 // A packed, uploaded batch: parents, chunks, value and statistics buffers.
@@ -358,6 +422,12 @@ struct BatchPlan {
     HistResult hist;
     bool need_hist = false;
     float fit_ms = 0.f, hist_ms = 0.f;       // device time of the last run
+    long long smem_cap = 0;
+    cudaGraphExec_t gexec = nullptr;         // captured fit stage (dressx_batch_capture)
+    ~BatchPlan()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+    }
 };
 
 Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
@@ -402,33 +472,16 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
         nranks += (long long)p->ranks.size();
         if (p->ms_host) ms_total += p->total * (long long)p->E;
     }
-    Tune tu = pick_tune(maxE, maxN, M, *en.cfg);
+    Tune tu = pick_tune(maxE, maxN, M, maxk, *en.cfg);
     BatchLaunch &L = P.L;
-    L.gsize = tu.gsize;
     L.maxE = maxE;
     L.maxN = maxN;
     L.maxk = maxk;
     L.M = M;
     L.parent_bytes = maxbytes;
-    // shrink the group count until parent + group states fit; drop staging last
-    L.stage = 1;
-    L.groups = tu.groups;
-    while (L.groups > 1 && (long long)batch_smem_bytes(L) > smem_cap) --L.groups;
-    if ((long long)batch_smem_bytes(L) > smem_cap) {
-        L.stage = 0;
-        L.groups = tu.groups;
-        while (L.groups > 1 && (long long)batch_smem_bytes(L) > smem_cap) --L.groups;
-    }
-    if ((long long)batch_smem_bytes(L) > smem_cap)
+    P.smem_cap = smem_cap;
+    if (!shape_launch(L, tu, smem_cap))
         return Status::Err(DRESSX_EUNSUPPORTED, "subgraph state exceeds shared memory");
-    if (L.stage && L.groups * 2 < tu.groups) {
-        // staging leaves too few groups: read parents from L2 instead
-        BatchLaunch L2 = L;
-        L2.stage = 0;
-        L2.groups = tu.groups;
-        while (L2.groups > 1 && (long long)batch_smem_bytes(L2) > smem_cap) --L2.groups;
-        if (L2.groups > L.groups) L = L2;
-    }
 
     // pack parents
     std::vector<unsigned char> hbytes((size_t)arena);
@@ -448,12 +501,8 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
         if (p->T) std::memcpy(b + PL.pairs, p->pairs.data(), (size_t)p->T * 8);
         hranks.insert(hranks.end(), p->ranks.begin(), p->ranks.end());
     }
-    // chunks: a few rounds of subgraphs per CTA visit
     std::vector<Chunk> &chunks = P.chunks;
-    const int chunk_items = 4 * L.groups;
-    for (size_t i = 0; i < ps.size(); ++i)
-        for (long long f = 0; f < ps[i]->items; f += chunk_items)
-            chunks.push_back({(int)i, (int)std::min<long long>(chunk_items, ps[i]->items - f), f});
+    build_chunks(ps, L.groups, -1, chunks);
 
     const int nreq = (int)ps.size();
     DevBuf<unsigned char> &d_pdata = P.d_pdata;
@@ -513,16 +562,29 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
 
 // Device work of a planned batch: all fits, then the histograms (left in
 // device memory).  Can be repeated; each run starts from the same inputs.
+// The fit stage: counters reset and the batch kernel.  It allocates nothing
+// and never synchronises, so it can be captured into a CUDA graph.
+Status enqueue_fit(BatchPlan &P, cudaStream_t st, int sms)
+{
+    const int nreq = (int)P.ps.size();
+    DRESS_CUDA_TRY(cudaMemsetAsync(P.d_stats.get(), 0, ST_WORDS * (size_t)nreq * sizeof(unsigned long long), st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(P.d_counter.get(), 0, sizeof(int), st));
+    return launch_batch(P.L, sms, st);
+}
+
 Status exec_batched(BatchPlan &P, const Ctx &en)
 {
     cudaStream_t st = en.st;
     const int nreq = (int)P.ps.size();
-    DRESS_CUDA_TRY(cudaMemsetAsync(P.d_stats.get(), 0, ST_WORDS * (size_t)nreq * sizeof(unsigned long long), st));
-    DRESS_CUDA_TRY(cudaMemsetAsync(P.d_counter.get(), 0, sizeof(int), st));
     cudaEvent_t ev[3];
     for (auto &e : ev) DRESS_CUDA_TRY(cudaEventCreate(&e));
     DRESS_CUDA_TRY(cudaEventRecord(ev[0], st));
-    DRESS_TRY(launch_batch(P.L, en.num_sms, st));
+    if (P.gexec) {
+        count_launch();
+        DRESS_CUDA_TRY(cudaGraphLaunch(P.gexec, st));
+    } else {
+        DRESS_TRY(enqueue_fit(P, st, en.num_sms));
+    }
     DRESS_CUDA_TRY(cudaEventRecord(ev[1], st));
     P.stats.assign(ST_WORDS * (size_t)nreq, 0);
     DRESS_CUDA_TRY(counted_memcpy(P.stats.data(), P.d_stats.get(), P.stats.size() * sizeof(unsigned long long),
@@ -571,6 +633,117 @@ Status collect_batched(BatchPlan &P, const Ctx &en)
                 o += n;
             }
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return Status::Ok();
+}
+
+// Autotuner: times the fit stage on the first subgraphs of the batch for
+// every group size whose state fits shared memory, records the fastest for
+// this size class (later batches of the class are planned with it) and
+// re-plans this batch with it.
+Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<float> *rates)
+{
+    cudaStream_t st = en.st;
+    long long total = 0;
+    for (Prep *p : P.ps) total += p->items;
+    if (total == 0) return Status::Ok();
+    const long long limit = total <= 3 * 16384 ? total : std::max<long long>(16384, total / 10);
+    const int cands[4] = {32, 64, 128, 256};
+    DevBuf<Chunk> d_try;
+    cudaEvent_t e0, e1;
+    DRESS_CUDA_TRY(cudaEventCreate(&e0));
+    DRESS_CUDA_TRY(cudaEventCreate(&e1));
+    int best = -1;
+    double best_rate = 0.0;
+    Status err;
+    for (int gs : cands) {
+        Tune tu{gs, gs == 32 ? 16 : std::min(15, 512 / gs)};
+        BatchLaunch L = P.L;
+        if (!shape_launch(L, tu, P.smem_cap)) {
+            if (rates) rates->push_back(0.f);
+            continue;
+        }
+        std::vector<Chunk> ch;
+        build_chunks(P.ps, L.groups, limit, ch);
+        long long items = 0;
+        for (const Chunk &c : ch) items += c.count;
+        err = d_try.alloc(ch.size(), st);
+        if (!err.ok()) break;
+        if (cudaMemcpyAsync(d_try.get(), ch.data(), ch.size() * sizeof(Chunk), cudaMemcpyHostToDevice, st) != cudaSuccess) {
+            err = Status::Err(DRESSX_ECUDA, "autotune: chunk upload failed");
+            break;
+        }
+        L.chunks = d_try.get();
+        L.nchunks = (int)ch.size();
+        float ms = 0.f;
+        for (int rep = 0; rep < 2; ++rep) {          // the first run is untimed
+            cudaMemsetAsync(P.d_stats.get(), 0, ST_WORDS * P.ps.size() * sizeof(unsigned long long), st);
+            cudaMemsetAsync(P.d_counter.get(), 0, sizeof(int), st);
+            cudaEventRecord(e0, st);
+            err = launch_batch(L, en.num_sms, st);
+            if (!err.ok()) break;
+            cudaEventRecord(e1, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) {
+                err = Status::Err(DRESSX_ECUDA, "autotune: run failed");
+                break;
+            }
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        if (!err.ok()) break;
+        const double rate = ms > 0.f ? (double)items / ms : 0.0;
+        if (rates) rates->push_back((float)rate);
+        if (rate > best_rate) {
+            best_rate = rate;
+            best = gs;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    DRESS_TRY(err);
+    if (best < 0) return Status::Err(DRESSX_EUNSUPPORTED, "autotune: no group size fits");
+    {
+        std::lock_guard<std::mutex> lk(g_tuned_mu);
+        g_tuned[tune_key(P.L.maxE, P.L.maxN, P.L.M, P.L.maxk)] = best;
+    }
+    Tune tu{best, best == 32 ? 16 : std::min(15, 512 / best)};
+    if (!shape_launch(P.L, tu, P.smem_cap)) return Status::Err(DRESSX_EUNSUPPORTED, "autotune: re-plan failed");
+    build_chunks(P.ps, P.L.groups, -1, P.chunks);
+    DRESS_TRY(P.d_chunks.alloc(P.chunks.size(), st));
+    DRESS_CUDA_TRY(counted_memcpy(P.d_chunks.get(), P.chunks.data(), P.chunks.size() * sizeof(Chunk),
+                                   cudaMemcpyHostToDevice, st));
+    P.L.chunks = P.d_chunks.get();
+    P.L.nchunks = (int)P.chunks.size();
+    if (P.gexec) {                       // the captured stage has the old schedule
+        cudaGraphExecDestroy(P.gexec);
+        P.gexec = nullptr;
+    }
+    DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    if (best_out) *best_out = best;
+    return Status::Ok();
+}
+
+// Captures the fit stage into a CUDA graph that exec_batched replays.
+Status capture_batched(BatchPlan &P, const Ctx &en)
+{
+    if (P.gexec) {
+        cudaGraphExecDestroy(P.gexec);
+        P.gexec = nullptr;
+    }
+    DRESS_CUDA_TRY(cudaStreamSynchronize(en.st));
+    cudaGraph_t g = nullptr;
+    DRESS_CUDA_TRY(cudaStreamBeginCapture(en.st, cudaStreamCaptureModeThreadLocal));
+    Status s = enqueue_fit(P, en.st, en.num_sms);
+    cudaError_t e = cudaStreamEndCapture(en.st, &g);
+    if (!s.ok() || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        return s.ok() ? Status::Err(DRESSX_ECUDA, std::string("stream capture: ") + cudaGetErrorString(e)) : s;
+    }
+    e = cudaGraphInstantiate(&P.gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        P.gexec = nullptr;
+        return Status::Err(DRESSX_ECUDA, std::string("graph instantiation: ") + cudaGetErrorString(e));
     }
     return Status::Ok();
 }
@@ -895,6 +1068,31 @@ int dressx_batch_run(dressx_batch_t *b)
     std::lock_guard<std::mutex> lk(en.mu);
     Status s = b->ptrs.empty() ? Status::Ok() : exec_batched(b->plan, en.ctx);
     b->ran = s.ok();
+    set_last_error(s);
+    return s.code;
+}
+
+int dressx_batch_autotune(dressx_batch_t *b, int *group_threads, float *rates)
+{
+    if (!b) return DRESSX_EINVAL;
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    std::vector<float> r;
+    int best = b->ptrs.empty() ? 0 : b->plan.L.gsize;
+    Status s = b->ptrs.empty() ? Status::Ok() : autotune_batched(b->plan, en.ctx, &best, &r);
+    if (group_threads) *group_threads = best;
+    if (rates)
+        for (int i = 0; i < 4; ++i) rates[i] = i < (int)r.size() ? r[(size_t)i] : 0.f;
+    set_last_error(s);
+    return s.code;
+}
+
+int dressx_batch_capture(dressx_batch_t *b)
+{
+    if (!b) return DRESSX_EINVAL;
+    Engine &en = engine();
+    std::lock_guard<std::mutex> lk(en.mu);
+    Status s = b->ptrs.empty() ? Status::Ok() : capture_batched(b->plan, en.ctx);
     set_last_error(s);
     return s.code;
 }

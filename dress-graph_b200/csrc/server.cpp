@@ -67,6 +67,9 @@ constexpr long long B200_SMEM_OPTIN = 232448;
 // buffer, and the sort / run-length scratch.
 constexpr long long HIST_BYTES_PER_VALUE = 56;
 
+// Largest whole-graph fit packed into batch launches.
+constexpr int PLAIN_BATCH_MAX_EDGES = 2048;
+
 // Threads per fit by edge count.
 int gsize_for(int E) { return E <= 640 ? 32 : E <= 2048 ? 64 : E <= 8192 ? 128 : 256; }
 
@@ -143,6 +146,10 @@ Status plan_request(p_dress_graph_t g, int kind, int k, long long smem_cap, bool
     bool batch = maxdeg <= 31 && batch_group_bytes(E, N, pl.k, gsize_for(E)) <= smem_cap - 1024 &&
                  batch_group_bytes(E, N, pl.k, gsize_for(E)) <= BATCH_GROUP_BYTES_MAX;
     if (kind != DRESSX_FIT) batch = batch && k >= 1 && k < N;
+    // a whole-graph fit in the batch kernel runs on one thread group (one
+    // SM); above a few thousand edges the single-graph fit, which spreads
+    // every sweep over the whole device, answers sooner
+    if (kind == DRESSX_FIT) batch = batch && E <= PLAIN_BATCH_MAX_EDGES;
     std::vector<int> ioff, pairs;
     if (batch) {
         bool dup = false;
@@ -298,7 +305,7 @@ Status Server::start(const dressx_server_config_t *c)
 {
     if (c) cfg = *c;
     else cfg.device = -1;
-    if (cfg.lanes <= 0) cfg.lanes = 2;
+    if (cfg.lanes <= 0) cfg.lanes = 4;
     if (cfg.launch_slots <= 0) cfg.launch_slots = 3;
     if (cfg.launch_work <= 0) cfg.launch_work = 1LL << 21;
     if (cfg.finishers <= 0) cfg.finishers = 2;

@@ -303,6 +303,18 @@ class Batch:
     def run(self):
         _check(lib().dressx_batch_run(self.handle))
 
+    def autotune(self):
+        """Measure 32/64/128/256 threads per subgraph on a sample, keep the
+        fastest.  Returns (threads, {threads: sampled fits per ms})."""
+        gt = ctypes.c_int()
+        rates = (ctypes.c_float * 4)()
+        _check(lib().dressx_batch_autotune(self.handle, ctypes.byref(gt), rates))
+        return gt.value, {t: float(r) for t, r in zip((32, 64, 128, 256), rates)}
+
+    def capture(self):
+        """Capture the fit stage into a CUDA graph replayed by ``run()``."""
+        _check(lib().dressx_batch_capture(self.handle))
+
     def fetch(self):
         _check(lib().dressx_batch_fetch(self.handle))
         out = []

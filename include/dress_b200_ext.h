@@ -106,6 +106,17 @@ typedef struct dressx_batch dressx_batch_t;
 int  dressx_batch_create(dressx_hist_request_t *reqs, int n, dressx_batch_t **out);
 /* All fits and histograms on the device; results stay in device memory. */
 int  dressx_batch_run(dressx_batch_t *b);
+/* Autotuner: runs the batch kernel on a sample of this batch's subgraphs
+ * with 32, 64, 128 and 256 threads per subgraph (each where one subgraph's
+ * state fits shared memory), keeps the fastest for the batch's size class --
+ * batches of that class planned later in the process start from it -- and
+ * re-plans this batch with it.  *group_threads gets the winner, rates[4]
+ * (nullable) the sampled subgraph-fits per ms of each candidate (0 = did not
+ * fit). */
+int  dressx_batch_autotune(dressx_batch_t *b, int *group_threads, float *rates);
+/* Captures the fit stage (counter resets and the batch kernel) into a CUDA
+ * graph; later dressx_batch_run calls replay it with one launch. */
+int  dressx_batch_capture(dressx_batch_t *b);
 /* Copies the last run's histograms (and multisets) into the requests. */
 int  dressx_batch_fetch(dressx_batch_t *b);
 /* Totals of the last run: subgraphs fitted, sweeps, live-edge updates. */
@@ -168,7 +179,8 @@ int dressx_hist_merge(const int64_t *const *flats, const int64_t *lens, int n, i
  *     the server's own memory pool (an arena that keeps its memory between
  *     requests) until they complete;
  *   - continuous batching: small requests (every row of at most 31
- *     neighbours, state within shared memory) are cut into slices and packed
+ *     neighbours, state within shared memory; whole-graph fits up to 2048
+ *     edges) are cut into slices and packed
  *     into short persistent batch launches, a few in flight at once; a
  *     request that arrives while launches run joins the next launch, every
  *     waiting request gets a share of each launch, and a request completes as
@@ -185,7 +197,7 @@ typedef struct dressx_server_config_t {
     int     device;               /* CUDA device ordinal; -1 = current        */
     size_t  memory_budget_bytes;  /* admission budget; 0 = 120 GiB, at most
                                      90% of the device memory free at create */
-    int     lanes;                /* concurrent large requests; 0 = 2          */
+    int     lanes;                /* concurrent large requests; 0 = 4          */
     int     launch_slots;         /* batch launches in flight; 0 = 3           */
     int64_t launch_work;          /* edge-subgraph units per batch launch
                                      (sum of edges over its fits); 0 = 2^21   */

@@ -165,3 +165,30 @@ def test_prepared_batch_reruns_match(oracle_port):
     b.close()
     for g in objs:
         g.close()
+
+
+@pytest.mark.parametrize("kind,k", [(db.DELTA, 2), (db.NABLA, 1)])
+def test_autotuned_and_captured_batch_matches(kind, k):
+    """Autotuning re-plans the batch (threads per subgraph, groups, chunks)
+    and capturing replays the fit stage from a CUDA graph: the histograms stay
+    those of the one-shot call."""
+    gs = [graphs.random_regular(40, 10, seed=s) for s in (1, 2, 3)]
+    objs = [db.Graph(n, U, V) for n, U, V in gs]
+    expect = [r[0] for r in db.hist_requests(objs, kind, k)]
+    b = db.Batch(objs, kind, k)
+    best, rates = b.autotune()
+    assert best in (32, 64, 128, 256) and rates[best] == max(rates.values()) > 0
+    b.run()
+    for x, y in zip(b.fetch(), expect):
+        np.testing.assert_array_equal(x, y)
+    b.capture()
+    for _ in range(2):
+        b.run()
+        for x, y in zip(b.fetch(), expect):
+            np.testing.assert_array_equal(x, y)
+    from math import comb, perm
+    n_sub = sum(comb(n, k) if kind == db.DELTA else perm(n, k) for n, _, _ in gs)
+    assert b.stats()["fits"] == n_sub
+    b.close()
+    for g in objs:
+        g.close()

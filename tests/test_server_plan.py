@@ -34,11 +34,20 @@ def test_hubs_and_trivial_orders_take_a_lane():
 
 
 def test_state_beyond_shared_memory_takes_a_lane():
-    # 4-regular with 20000 edges: rows are short but one fit's state
+    # 4-regular with 20000 edges: rows are short but one subgraph's state
     # (2 x 20000 edge values + norms) exceeds shared memory
     n, U, V = graphs.random_regular(10000, 4, seed=4)
     with db.Graph(n, U, V) as g:
+        assert db.estimate(g, db.DELTA, 1)[1] == db.PATH_LANE
+
+
+def test_larger_whole_graph_fits_take_a_lane():
+    # 3000 edges: its Delta^1 subgraphs are batched, the whole-graph fit runs
+    # on the single-graph engine, which spreads each sweep over the device
+    n, U, V = graphs.random_regular(1000, 6, seed=4)
+    with db.Graph(n, U, V) as g:
         assert db.estimate(g, db.FIT)[1] == db.PATH_LANE
+        assert db.estimate(g, db.DELTA, 1)[1] == db.PATH_BATCH
 
 
 def test_estimate_grows_with_the_graph():
