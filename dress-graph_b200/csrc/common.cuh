@@ -140,7 +140,9 @@ __device__ __forceinline__ void block_max_to(unsigned long long *dst, double v)
         int nw = (blockDim.x + 31) >> 5;
         v = lane < nw ? red[lane] : 0.0;
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (lane == 0 && v > 0.0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+        // most blocks do not raise the running maximum: look before the atomic
+        if (lane == 0 && v > 0.0 && v > __longlong_as_double((long long)*(volatile unsigned long long *)dst))
+            atomicMax(dst, (unsigned long long)__double_as_longlong(v));
     }
 }
 

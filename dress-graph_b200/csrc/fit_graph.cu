@@ -205,28 +205,29 @@ __global__ void k_copy_i64(long long n, const long long *src, unsigned long long
 }
 
 // ---- binning (terms per item) and renumbering ----
-__global__ void k_bin_count(int n, const int *len, int add, int *bin_cnt)
+__global__ void k_bin_count(int n, const int *len, int *bin_cnt)
 {
-    __shared__ int sc[NB];
-    if (threadIdx.x < NB) sc[threadIdx.x] = 0;
+    __shared__ int sc[NF];
+    for (int f = threadIdx.x; f < NF; f += blockDim.x) sc[f] = 0;
     __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        atomicAdd(&sc[bin_of((long long)len[i] + add)], 1);
+        atomicAdd(&sc[fine_of((long long)len[i])], 1);
     __syncthreads();
-    if (threadIdx.x < NB && sc[threadIdx.x]) atomicAdd(&bin_cnt[threadIdx.x], sc[threadIdx.x]);
+    for (int f = threadIdx.x; f < NF; f += blockDim.x)
+        if (sc[f]) atomicAdd(&bin_cnt[f], sc[f]);
 }
 
-// Scatter items into their bins; lanes of a warp that share a bin take
-// consecutive slots (one atomic per group), which keeps neighbouring items
-// neighbours.
-__global__ void k_bin_scatter(int n, const int *len, int add, int *cursor, int *perm, int *inv)
+// Scatter items to their fine keys' ranges; lanes of a warp that share a key
+// take consecutive slots (one atomic per group), which keeps neighbouring
+// items neighbours.
+__global__ void k_bin_scatter(int n, const int *len, int *cursor, int *perm, int *inv)
 {
     int lane = threadIdx.x & 31;
     for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
         int i = i0 + threadIdx.x;
         unsigned active = __ballot_sync(0xffffffffu, i < n);
         if (i < n) {
-            int b = bin_of((long long)len[i] + add);
+            int b = fine_of((long long)len[i]);
             unsigned peers = __match_any_sync(active, b);
             int leader = __ffs(peers) - 1;
             int base = 0;
@@ -450,31 +451,38 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
 
     // ---- bins and renumbering ---------------------------------------------------
     DevBuf<int> d_bc, d_vperm, d_vinv, d_eperm, d_einv;
-    DRESS_TRY(d_bc.alloc(4 * NB, st));
+    DRESS_TRY(d_bc.alloc(4 * NF, st));
     DRESS_TRY(d_vperm.alloc((size_t)N, st));
     DRESS_TRY(d_vinv.alloc((size_t)N, st));
     DRESS_TRY(d_eperm.alloc((size_t)E, st));
     DRESS_TRY(d_einv.alloc((size_t)E, st));
-    DRESS_CUDA_TRY(cudaMemsetAsync(d_bc.get(), 0, 4 * NB * sizeof(int), st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_bc.get(), 0, 4 * NF * sizeof(int), st));
     const int vg = (int)grid_for(N, 256, 32 * sms);
-    count_launch(), k_bin_count<<<vg, 256, 0, st>>>(N, d_deg.get(), 0, d_bc.get());
-    count_launch(), k_bin_count<<<eg, 256, 0, st>>>(E, d_cnt.get(), 0, d_bc.get() + NB);
-    int bc[2 * NB];
-    DRESS_CUDA_TRY(counted_memcpy(bc, d_bc.get(), sizeof(bc), cudaMemcpyDeviceToHost, st));
+    count_launch(), k_bin_count<<<vg, 256, 0, st>>>(N, d_deg.get(), d_bc.get());
+    count_launch(), k_bin_count<<<eg, 256, 0, st>>>(E, d_cnt.get(), d_bc.get() + NF);
+    std::vector<int> bc(2 * NF);
+    DRESS_CUDA_TRY(counted_memcpy(bc.data(), d_bc.get(), 2 * NF * sizeof(int), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     if (flags[0]) return Status::Err(DRESSX_EINVAL, "malformed intercept tables");
-    Bins vb, eb;
-    vb.start[0] = eb.start[0] = 0;
-    for (int b = 0; b < NB; ++b) {
-        vb.start[b + 1] = vb.start[b] + bc[b];
-        eb.start[b + 1] = eb.start[b] + bc[NB + b];
+    // fine ranges (cursors), then the coarse bins they make up
+    std::vector<int> cur(2 * NF);
+    cur[0] = 0;
+    cur[NF] = 0;
+    for (int f = 1; f < NF; ++f) {
+        cur[f] = cur[f - 1] + bc[f - 1];
+        cur[NF + f] = cur[NF + f - 1] + bc[NF + f - 1];
     }
-    int cur[2 * NB];
-    for (int b = 0; b < NB; ++b) { cur[b] = vb.start[b]; cur[NB + b] = eb.start[b]; }
-    DRESS_CUDA_TRY(counted_memcpy(d_bc.get() + 2 * NB, cur, sizeof(cur), cudaMemcpyHostToDevice, st));
-    count_launch(), k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), 0, d_bc.get() + 2 * NB, d_vperm.get(), d_vinv.get());
-    count_launch(), k_bin_scatter<<<eg, 256, 0, st>>>(E, d_cnt.get(), 0, d_bc.get() + 3 * NB, d_eperm.get(), d_einv.get());
+    Bins vb, eb;
+    for (int b = 0; b < NB; ++b) {
+        vb.start[b] = cur[fine_first(b)];
+        eb.start[b] = cur[NF + fine_first(b)];
+    }
+    vb.start[NB] = N;
+    eb.start[NB] = E;
+    DRESS_CUDA_TRY(counted_memcpy(d_bc.get() + 2 * NF, cur.data(), 2 * NF * sizeof(int), cudaMemcpyHostToDevice, st));
+    count_launch(), k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), d_bc.get() + 2 * NF, d_vperm.get(), d_vinv.get());
+    count_launch(), k_bin_scatter<<<eg, 256, 0, st>>>(E, d_cnt.get(), d_bc.get() + 3 * NF, d_eperm.get(), d_einv.get());
     // block items largest first, so the longest sequential sums start first
     {
         struct Seg { int *perm, *inv; const int *len; int b0, b1; };
@@ -602,7 +610,10 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     s.eu = d_eu.get(); s.ev = d_ev.get();
     s.w = uniform ? nullptr : d_wi.get();
     s.wc = wc;
-    s.nw = d_nwi.get();
+    bool unit_nw = true;                       // NULL vertex weights mean all 1.0
+    if (g->NW)
+        for (int i = 0; i < N && unit_nw; ++i) unit_nw = g->NW[i] == 1.0;
+    s.nw = unit_nw ? nullptr : d_nwi.get();
     s.ioff = d_ioff.get(); s.pairs = d_pairs.get();
     s.vd = d_vd.get(); s.maxd = d_maxd.get();
     s.eps = epsilon;
@@ -616,6 +627,28 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     s.bkey_v = d_bkey_v.get(); s.bkey_e = d_bkey_e.get();
     s.bofs_v = d_bofs_v.get(); s.bofs_e = d_bofs_e.get();
     s.bv0 = vb.start[BBLOCK]; s.be0 = eb.start[BBLOCK];
+    // sorted-term slots of the streamed items (queued ones are sorted into them)
+    DevBuf<double> d_skey, d_tkey;
+    {
+        long long lim[4] = {0, 0, 0, 0};
+        if (vb.has(BMED)) {
+            DRESS_CUDA_TRY(counted_memcpy(&lim[0], d_row_off.get() + vb.start[BMED], sizeof(long long),
+                                           cudaMemcpyDeviceToHost, st));
+            DRESS_CUDA_TRY(counted_memcpy(&lim[1], d_row_off.get() + vb.start[BMED + 1], sizeof(long long),
+                                           cudaMemcpyDeviceToHost, st));
+        }
+        if (eb.has(BMED)) {
+            DRESS_CUDA_TRY(counted_memcpy(&lim[2], d_ioff.get() + eb.start[BMED], sizeof(long long),
+                                           cudaMemcpyDeviceToHost, st));
+            DRESS_CUDA_TRY(counted_memcpy(&lim[3], d_ioff.get() + eb.start[BMED + 1], sizeof(long long),
+                                           cudaMemcpyDeviceToHost, st));
+        }
+        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+        DRESS_TRY(d_skey.alloc((size_t)std::max(1LL, lim[1] - lim[0]), st));
+        DRESS_TRY(d_tkey.alloc((size_t)std::max(1LL, lim[3] - lim[2]), st));
+        s.skey = d_skey.get(); s.sbase = lim[0];
+        s.tkey = d_tkey.get(); s.tbase = lim[2];
+    }
     LaunchCfg lc{sms, block_cap, vblock_cap, st, ctx.side, ctx.fork, ctx.join};
     double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + E};
     double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + E};

@@ -42,6 +42,25 @@ __host__ __device__ __forceinline__ int bin_of(long long n)
          : n <= BIG_CAP ? BBLOCK : BBIG;
 }
 
+// Fine keys of the renumbering: the coarse bins, with the streamed bin split
+// by exact term count, longest first -- neighbouring threads then run loops
+// of equal length, and the longest loops start first.
+constexpr int NF = BMED + (MED_CAP - 16) + 2;
+
+__host__ __device__ __forceinline__ int fine_of(long long n)
+{
+    const int b = bin_of(n);
+    if (b < BMED) return b;
+    if (b == BMED) return BMED + (MED_CAP - (int)n);
+    return BMED + (MED_CAP - 16) + (b - BBLOCK);
+}
+
+// first fine key of a coarse bin
+__host__ __device__ __forceinline__ int fine_first(int b)
+{
+    return b <= BMED ? b : BMED + (MED_CAP - 16) + (b - BBLOCK);
+}
+
 struct Sweep {
     int N, E, fwd;                 // fwd: FORWARD/BACKWARD self term
     const long long *row_off;      // [N+1] renumbered CSR rows
@@ -49,7 +68,7 @@ struct Sweep {
     const int *eu, *ev;            // [E]
     const double *w;               // [E] (weighted graphs)
     double wc;                     // the weight when all are equal
-    const double *nw;              // [N]
+    const double *nw;              // [N], or null when every vertex weight is 1.0
     const long long *ioff;         // [E+1]
     int2 *pairs;                   // [T]  common-neighbour edge pairs, kept in value order
     double *vd;                    // [N]
@@ -66,6 +85,8 @@ struct Sweep {
     double *bkey_v, *bkey_e;       // sorted terms of the block items, one slot per item
     const long long *bofs_v, *bofs_e;   // slot offsets, indexed from bv0 / be0
     int bv0, be0;                  // first block item (vertex, edge)
+    double *skey, *tkey;           // sorted terms of queued streamed items, at their
+    long long sbase, tbase;        // row slot / pair offset minus these bases
 };
 
 __device__ __forceinline__ bool skipped(const Sweep &s)
@@ -79,13 +100,19 @@ __device__ __forceinline__ double prod(const Sweep &s, int e)
     return UNIF ? dmul(s.wc, s.d[e]) : s.p[e];
 }
 
+// 4 * nw of a vertex (exactly 4.0 for unit weights)
+__device__ __forceinline__ double four_nw(const Sweep &s, int i)
+{
+    return s.nw ? dmul(4.0, s.nw[i]) : 4.0;
+}
+
 template <bool UNIF>
 __device__ __forceinline__ double self_term(const Sweep &s, int j, int u, int v)
 {
     double own = prod<UNIF>(s, j);
-    double a = dmul(4.0, s.nw[u]);
+    double a = four_nw(s, u);
     if (s.fwd) return dadd(a, own);
-    return dadd(dadd(a, dmul(4.0, s.nw[v])), dmul(2.0, own));
+    return dadd(dadd(a, four_nw(s, v)), dmul(2.0, own));
 }
 
 // edge value from its numerator; stores d_next (and p_next), returns |delta|
@@ -284,40 +311,42 @@ __device__ __forceinline__ void fix_order(double *keys, P *vals, int n, int tid,
 
 // ---- one thread per item (at most 16 stored terms) ----------------------------------
 
+// Grid-stride loops over a bounded grid: one convergence atomic per block,
+// not one per 128 items.
 template <int M, bool UNIF>
 __global__ void __launch_bounds__(128) k_vertex_thr(Sweep s, int begin, int end)
 {
     if (skipped(s)) return;
-    const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= end) return;
-    const double self = dmul(4.0, s.nw[i]);
-    if constexpr (M == 0) {
-        s.vd[i] = dsqrt(dadd(self, 0.0));
-    } else {
-        const long long b = s.row_off[i];
-        const int deg = (int)(s.row_off[i + 1] - b);
-        double a[M];
-        int id[M];
+    for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
+        const double self = four_nw(s, i);
+        if constexpr (M == 0) {
+            s.vd[i] = dsqrt(dadd(self, 0.0));
+        } else {
+            const long long b = s.row_off[i];
+            const int deg = (int)(s.row_off[i + 1] - b);
+            double a[M];
+            int id[M];
 #pragma unroll
-        for (int k = 0; k < M; ++k) {
-            if (k < deg) {
-                id[k] = s.row_eid[b + k];
-                a[k] = prod<UNIF>(s, id[k]);
-            } else {
-                id[k] = -1;
-                a[k] = DRESS_INF;
+            for (int k = 0; k < M; ++k) {
+                if (k < deg) {
+                    id[k] = s.row_eid[b + k];
+                    a[k] = prod<UNIF>(s, id[k]);
+                } else {
+                    id[k] = -1;
+                    a[k] = DRESS_INF;
+                }
             }
-        }
-        bool sorted = true;
+            bool sorted = true;
 #pragma unroll
-        for (int k = 0; k + 1 < M; ++k) sorted &= !(a[k + 1] < a[k]);
-        if (!sorted) {
-            sort_kv<M>(a, id);
+            for (int k = 0; k + 1 < M; ++k) sorted &= !(a[k + 1] < a[k]);
+            if (!sorted) {
+                sort_kv<M>(a, id);
 #pragma unroll
-            for (int k = 0; k < M; ++k)
-                if (k < deg) s.row_eid[b + k] = id[k];
+                for (int k = 0; k < M; ++k)
+                    if (k < deg) s.row_eid[b + k] = id[k];
+            }
+            s.vd[i] = dsqrt(kbn_merge_regs<M>(a, deg, self));
         }
-        s.vd[i] = dsqrt(kbn_merge_regs<M>(a, deg, self));
     }
 }
 
@@ -325,9 +354,8 @@ template <int M, bool UNIF>
 __global__ void __launch_bounds__(128) k_edge_thr(Sweep s, int begin, int end)
 {
     if (skipped(s)) return;
-    const int j = begin + blockIdx.x * blockDim.x + threadIdx.x;
     double delta = 0.0;
-    if (j < end) {
+    for (int j = begin + blockIdx.x * blockDim.x + threadIdx.x; j < end; j += gridDim.x * blockDim.x) {
         const int u = s.eu[j], v = s.ev[j];
         const double self = self_term<UNIF>(s, j, u, v);
         double num;
@@ -359,7 +387,7 @@ __global__ void __launch_bounds__(128) k_edge_thr(Sweep s, int begin, int end)
             }
             num = kbn_merge_regs<M>(a, nc, self);
         }
-        delta = finish_edge<UNIF>(s, j, u, v, num);
+        delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, num));
     }
     block_max_to(&s.maxd[s.slot], delta);
 }
@@ -377,7 +405,7 @@ __global__ void __launch_bounds__(256) k_vertex_med(Sweep s, int begin, int end)
     for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const long long b = s.row_off[i];
         const int deg = (int)(s.row_off[i + 1] - b);
-        KbnStream ks(dmul(4.0, s.nw[i]));
+        KbnStream ks(four_nw(s, i));
         double prev = -DRESS_INF;
         bool ok = true;
         for (int k = 0; k < deg && ok; k += STREAM_D) {
@@ -457,8 +485,11 @@ __global__ void __launch_bounds__(256) k_vertex_med_sort(Sweep s)
         for (int k = lane; k + 1 < deg; k += 32) d += kb[k + 1] < kb[k];
         for (int o2 = 16; o2 > 0; o2 >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o2);
         fix_order(kb, pb, deg, lane, 32, WarpSync(), WarpAny(), far_from_sorted(d, deg));
-        for (int k = lane; k < deg; k += 32) s.row_eid[b + k] = pb[k];
-        if (lane == 0) s.vd[i] = dsqrt(kbn_merge_buf(kb, deg, dmul(4.0, s.nw[i])));
+        double *out = s.skey + (b - s.sbase);
+        for (int k = lane; k < deg; k += 32) {
+            s.row_eid[b + k] = pb[k];
+            out[k] = kb[k];
+        }
         __syncwarp();
     }
 }
@@ -468,7 +499,6 @@ __global__ void __launch_bounds__(256) k_edge_med_sort(Sweep s)
 {
     extern __shared__ __align__(16) unsigned char smw[];
     if (skipped(s)) return;
-    double delta = 0.0;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     double *kb = (double *)smw + (size_t)wid * MED_CAP;
     int2 *pb = (int2 *)((double *)smw + (size_t)nwarps * MED_CAP) + (size_t)wid * MED_CAP;
@@ -487,12 +517,42 @@ __global__ void __launch_bounds__(256) k_edge_med_sort(Sweep s)
         for (int k = lane; k + 1 < nc; k += 32) d += kb[k + 1] < kb[k];
         for (int o2 = 16; o2 > 0; o2 >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o2);
         fix_order(kb, pb, nc, lane, 32, WarpSync(), WarpAny(), far_from_sorted(d, nc));
-        for (int k = lane; k < nc; k += 32) s.pairs[o + k] = pb[k];
-        if (lane == 0) {
-            const int u = s.eu[j], v = s.ev[j];
-            delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_merge_buf(kb, nc, self_term<UNIF>(s, j, u, v))));
+        double *out = s.tkey + (o - s.tbase);
+        for (int k = lane; k < nc; k += 32) {
+            s.pairs[o + k] = pb[k];
+            out[k] = kb[k];
         }
         __syncwarp();
+    }
+}
+
+// one thread per queued item: the sequential sum of its sorted terms
+template <bool UNIF>
+__global__ void __launch_bounds__(128) k_vertex_med_sum(Sweep s)
+{
+    if (skipped(s)) return;
+    const int n_items = (int)s.qcount[0];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += gridDim.x * blockDim.x) {
+        const int i = s.qv[q];
+        const long long b = s.row_off[i];
+        const int deg = (int)(s.row_off[i + 1] - b);
+        s.vd[i] = dsqrt(kbn_merge_buf(s.skey + (b - s.sbase), deg, four_nw(s, i)));
+    }
+}
+
+template <bool UNIF>
+__global__ void __launch_bounds__(128) k_edge_med_sum(Sweep s)
+{
+    if (skipped(s)) return;
+    double delta = 0.0;
+    const int n_items = (int)s.qcount[1];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_items; q += gridDim.x * blockDim.x) {
+        const int j = s.qe[q];
+        const long long o = s.ioff[j];
+        const int nc = (int)(s.ioff[j + 1] - o);
+        const int u = s.eu[j], v = s.ev[j];
+        delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_merge_buf(s.tkey + (o - s.tbase), nc,
+                                                                       self_term<UNIF>(s, j, u, v))));
     }
     block_max_to(&s.maxd[s.slot], delta);
 }
@@ -534,7 +594,7 @@ __global__ void __launch_bounds__(512) k_vertex_block(Sweep s, int begin, int en
             for (int k = threadIdx.x; k < deg; k += blockDim.x) s.row_eid[b + k] = pb[k];
         }
         if (SUM_HERE) {
-            if (threadIdx.x == 0) s.vd[i] = dsqrt(kbn_merge_buf(kb, deg, dmul(4.0, s.nw[i])));
+            if (threadIdx.x == 0) s.vd[i] = dsqrt(kbn_merge_buf(kb, deg, four_nw(s, i)));
         } else if (inshm) {
             for (int k = threadIdx.x; k < deg; k += blockDim.x) slot[k] = kb[k];
         }
@@ -593,7 +653,7 @@ __global__ void __launch_bounds__(128) k_vertex_block_sum(Sweep s, int begin, in
     const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= end) return;
     const int deg = (int)(s.row_off[i + 1] - s.row_off[i]);
-    s.vd[i] = dsqrt(kbn_merge_buf(s.bkey_v + s.bofs_v[i - s.bv0], deg, dmul(4.0, s.nw[i])));
+    s.vd[i] = dsqrt(kbn_merge_buf(s.bkey_v + s.bofs_v[i - s.bv0], deg, four_nw(s, i)));
 }
 
 template <bool UNIF>
@@ -691,14 +751,17 @@ template <bool UNIF, bool EDGE>
 void launch_med(const Sweep &s, const Bins &b, const LaunchCfg &c)
 {
     if (!b.has(BMED)) return;
-    const unsigned g = grid_for(b.count(BMED), MED_THR, INT_MAX);
+    const unsigned g = grid_for(b.count(BMED), MED_THR, 8 * c.sms);
     const unsigned gq = grid_for(b.count(BMED), MED_THR / 32, 8 * c.sms);
+    const unsigned gs = grid_for(b.count(BMED), THR, 16 * c.sms);
     if (EDGE) {
         count_launch(), k_edge_med<UNIF><<<g, MED_THR, 0, c.st>>>(s, b.start[BMED], b.start[BMED + 1]);
         count_launch(), k_edge_med_sort<UNIF><<<gq, MED_THR, med_smem_edge(), c.st>>>(s);
+        count_launch(), k_edge_med_sum<UNIF><<<gs, THR, 0, c.st>>>(s);
     } else {
         count_launch(), k_vertex_med<UNIF><<<g, MED_THR, 0, c.st>>>(s, b.start[BMED], b.start[BMED + 1]);
         count_launch(), k_vertex_med_sort<UNIF><<<gq, MED_THR, med_smem_vertex(), c.st>>>(s);
+        count_launch(), k_vertex_med_sum<UNIF><<<gs, THR, 0, c.st>>>(s);
     }
 }
 
@@ -716,11 +779,11 @@ Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, const Launch
         launch_blocks<UNIF, false>(s, vb, c);
     }
     launch_med<UNIF, false>(s, vb, c);
-    if (vb.has(B16)) count_launch(), k_vertex_thr<16, UNIF><<<grid_for(vb.count(B16), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B16], vb.start[B16 + 1]);
-    if (vb.has(B8)) count_launch(), k_vertex_thr<8, UNIF><<<grid_for(vb.count(B8), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B8], vb.start[B8 + 1]);
-    if (vb.has(B4)) count_launch(), k_vertex_thr<4, UNIF><<<grid_for(vb.count(B4), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B4], vb.start[B4 + 1]);
-    if (vb.has(B2)) count_launch(), k_vertex_thr<2, UNIF><<<grid_for(vb.count(B2), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B2], vb.start[B2 + 1]);
-    if (vb.has(B0)) count_launch(), k_vertex_thr<0, UNIF><<<grid_for(vb.count(B0), THR, INT_MAX), THR, 0, c.st>>>(s, vb.start[B0], vb.start[B0 + 1]);
+    if (vb.has(B16)) count_launch(), k_vertex_thr<16, UNIF><<<grid_for(vb.count(B16), THR, 16 * c.sms), THR, 0, c.st>>>(s, vb.start[B16], vb.start[B16 + 1]);
+    if (vb.has(B8)) count_launch(), k_vertex_thr<8, UNIF><<<grid_for(vb.count(B8), THR, 16 * c.sms), THR, 0, c.st>>>(s, vb.start[B8], vb.start[B8 + 1]);
+    if (vb.has(B4)) count_launch(), k_vertex_thr<4, UNIF><<<grid_for(vb.count(B4), THR, 16 * c.sms), THR, 0, c.st>>>(s, vb.start[B4], vb.start[B4 + 1]);
+    if (vb.has(B2)) count_launch(), k_vertex_thr<2, UNIF><<<grid_for(vb.count(B2), THR, 16 * c.sms), THR, 0, c.st>>>(s, vb.start[B2], vb.start[B2 + 1]);
+    if (vb.has(B0)) count_launch(), k_vertex_thr<0, UNIF><<<grid_for(vb.count(B0), THR, 16 * c.sms), THR, 0, c.st>>>(s, vb.start[B0], vb.start[B0 + 1]);
     if (vside) {
         DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
         DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
@@ -732,11 +795,11 @@ Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, const Launch
         launch_blocks<UNIF, true>(s, eb, c);
     }
     launch_med<UNIF, true>(s, eb, c);
-    if (eb.has(B16)) count_launch(), k_edge_thr<16, UNIF><<<grid_for(eb.count(B16), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B16], eb.start[B16 + 1]);
-    if (eb.has(B8)) count_launch(), k_edge_thr<8, UNIF><<<grid_for(eb.count(B8), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B8], eb.start[B8 + 1]);
-    if (eb.has(B4)) count_launch(), k_edge_thr<4, UNIF><<<grid_for(eb.count(B4), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B4], eb.start[B4 + 1]);
-    if (eb.has(B2)) count_launch(), k_edge_thr<2, UNIF><<<grid_for(eb.count(B2), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B2], eb.start[B2 + 1]);
-    if (eb.has(B0)) count_launch(), k_edge_thr<0, UNIF><<<grid_for(eb.count(B0), THR, INT_MAX), THR, 0, c.st>>>(s, eb.start[B0], eb.start[B0 + 1]);
+    if (eb.has(B16)) count_launch(), k_edge_thr<16, UNIF><<<grid_for(eb.count(B16), THR, 16 * c.sms), THR, 0, c.st>>>(s, eb.start[B16], eb.start[B16 + 1]);
+    if (eb.has(B8)) count_launch(), k_edge_thr<8, UNIF><<<grid_for(eb.count(B8), THR, 16 * c.sms), THR, 0, c.st>>>(s, eb.start[B8], eb.start[B8 + 1]);
+    if (eb.has(B4)) count_launch(), k_edge_thr<4, UNIF><<<grid_for(eb.count(B4), THR, 16 * c.sms), THR, 0, c.st>>>(s, eb.start[B4], eb.start[B4 + 1]);
+    if (eb.has(B2)) count_launch(), k_edge_thr<2, UNIF><<<grid_for(eb.count(B2), THR, 16 * c.sms), THR, 0, c.st>>>(s, eb.start[B2], eb.start[B2 + 1]);
+    if (eb.has(B0)) count_launch(), k_edge_thr<0, UNIF><<<grid_for(eb.count(B0), THR, 16 * c.sms), THR, 0, c.st>>>(s, eb.start[B0], eb.start[B0 + 1]);
     if (eside) {
         DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
         DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
