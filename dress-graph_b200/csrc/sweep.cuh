@@ -23,6 +23,7 @@
 //   slab).  The block items are split at BIG_CAP so that the smaller ones run
 //   several blocks per SM.
 #pragma once
+#include <algorithm>
 #include <climits>
 
 #include "common.cuh"
@@ -199,6 +200,106 @@ struct KbnStream {
         return dadd(s, c);
     }
 };
+
+// Same over an ascending run in global memory: the self term's rank by
+// binary search, then 32-term windows, the next window's loads in flight
+// while the current one is summed, so the chain does not wait on L2 or HBM.
+__device__ __forceinline__ double kbn_merge_stream(const double *__restrict__ a, int n, double x)
+{
+    constexpr int W = 32;
+    int lo = 0, hi = n;                      // first index with a[idx] >= x
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    const int pos = lo;
+    // s = -0.0, c = +0.0: the first step then leaves s = that term, c = +0.0
+    // exactly, as starting the sum at it does (for every finite term, zeros
+    // of either sign included)
+    double s = -0.0, c = 0.0;
+    int i = 0;
+    for (; i < pos; ++i) kbn_step(s, c, a[i]);
+    kbn_step(s, c, x);
+    if (i + W <= n) {
+        double cur[W], nxt[W];
+#pragma unroll
+        for (int t = 0; t < W; ++t) cur[t] = a[i + t];
+        while (i + 2 * W <= n) {
+#pragma unroll
+            for (int t = 0; t < W; ++t) nxt[t] = a[i + W + t];
+#pragma unroll
+            for (int t = 0; t < W; ++t) kbn_step(s, c, cur[t]);
+#pragma unroll
+            for (int t = 0; t < W; ++t) cur[t] = nxt[t];
+            i += W;
+        }
+#pragma unroll
+        for (int t = 0; t < W; ++t) kbn_step(s, c, cur[t]);
+        i += W;
+    }
+    for (; i < n; ++i) kbn_step(s, c, a[i]);
+    return dadd(s, c);
+}
+
+// Sorted KBN of the n terms term(0..n) taken in stored order, with x merged
+// at its rank, while checking that the terms ascend; false when they do not
+// (the sum is then unusable).  Windows of W terms, the next window gathered
+// while the current one is summed; x is looked for once per window.
+template <int W, class Term>
+__device__ __forceinline__ bool kbn_stream_checked(int n, double x, Term term, double &out)
+{
+    double s = -0.0, c = 0.0, prev = -DRESS_INF;     // see kbn_merge_stream
+    bool ins = false, ok = true;
+    int i = 0;
+    if (n >= W) {
+        double cur[W], nxt[W];
+#pragma unroll
+        for (int t = 0; t < W; ++t) cur[t] = term(t);
+        for (;;) {
+            const bool more = i + 2 * W <= n;
+            if (more) {
+#pragma unroll
+                for (int t = 0; t < W; ++t) nxt[t] = term(i + W + t);
+            }
+            bool o = !(cur[0] < prev);
+#pragma unroll
+            for (int t = 0; t + 1 < W; ++t) o &= !(cur[t + 1] < cur[t]);
+            ok &= o;
+            prev = cur[W - 1];
+            if (!ins && !(cur[W - 1] < x)) {
+#pragma unroll
+                for (int t = 0; t < W; ++t) {
+                    if (!ins && !(cur[t] < x)) {
+                        kbn_step(s, c, x);
+                        ins = true;
+                    }
+                    kbn_step(s, c, cur[t]);
+                }
+            } else {
+#pragma unroll
+                for (int t = 0; t < W; ++t) kbn_step(s, c, cur[t]);
+            }
+            i += W;
+            if (!more) break;
+#pragma unroll
+            for (int t = 0; t < W; ++t) cur[t] = nxt[t];
+        }
+    }
+    for (; i < n; ++i) {
+        const double v = term(i);
+        ok &= !(v < prev);
+        prev = v;
+        if (!ins && !(v < x)) {
+            kbn_step(s, c, x);
+            ins = true;
+        }
+        kbn_step(s, c, v);
+    }
+    if (!ins) kbn_step(s, c, x);
+    out = dadd(s, c);
+    return ok;
+}
 
 // Same over an ascending buffer (one thread).
 __device__ __forceinline__ double kbn_merge_buf(const double *a, int n, double x)
@@ -396,7 +497,7 @@ __global__ void __launch_bounds__(128) k_edge_thr(Sweep s, int begin, int end)
 // The terms are gathered STREAM_D at a time (independent loads in flight),
 // summed in stored order while the order is checked; an item met out of
 // order is queued for k_*_med_sort, which sorts it and finishes it.
-constexpr int STREAM_D = 8;
+constexpr int STREAM_D = 16;
 
 template <bool UNIF>
 __global__ void __launch_bounds__(256) k_vertex_med(Sweep s, int begin, int end)
@@ -405,24 +506,12 @@ __global__ void __launch_bounds__(256) k_vertex_med(Sweep s, int begin, int end)
     for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const long long b = s.row_off[i];
         const int deg = (int)(s.row_off[i + 1] - b);
-        KbnStream ks(four_nw(s, i));
-        double prev = -DRESS_INF;
-        bool ok = true;
-        for (int k = 0; k < deg && ok; k += STREAM_D) {
-            double v[STREAM_D];
-#pragma unroll
-            for (int t = 0; t < STREAM_D; ++t)
-                if (k + t < deg) v[t] = prod<UNIF>(s, s.row_eid[b + k + t]);
-#pragma unroll
-            for (int t = 0; t < STREAM_D; ++t) {
-                if (k + t < deg && ok) {
-                    if (v[t] < prev) ok = false;
-                    else { prev = v[t]; ks.push(v[t]); }
-                }
-            }
-        }
-        if (ok) s.vd[i] = dsqrt(ks.finish());
-        else s.qv[atomicAdd(&s.qcount[0], 1u)] = i;
+        const int *rows = s.row_eid + b;
+        double sum;
+        if (kbn_stream_checked<STREAM_D>(deg, four_nw(s, i), [&](int k) { return prod<UNIF>(s, rows[k]); }, sum))
+            s.vd[i] = dsqrt(sum);
+        else
+            s.qv[atomicAdd(&s.qcount[0], 1u)] = i;
     }
 }
 
@@ -435,27 +524,15 @@ __global__ void __launch_bounds__(256) k_edge_med(Sweep s, int begin, int end)
         const int u = s.eu[j], v = s.ev[j];
         const long long o = s.ioff[j];
         const int nc = (int)(s.ioff[j + 1] - o);
-        KbnStream ks(self_term<UNIF>(s, j, u, v));
-        double prev = -DRESS_INF;
-        bool ok = true;
-        for (int k = 0; k < nc && ok; k += STREAM_D) {
-            double x[STREAM_D];
-#pragma unroll
-            for (int t = 0; t < STREAM_D; ++t)
-                if (k + t < nc) {
-                    const int2 pr = s.pairs[o + k + t];
-                    x[t] = dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
-                }
-#pragma unroll
-            for (int t = 0; t < STREAM_D; ++t) {
-                if (k + t < nc && ok) {
-                    if (x[t] < prev) ok = false;
-                    else { prev = x[t]; ks.push(x[t]); }
-                }
-            }
-        }
-        if (ok) delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, ks.finish()));
-        else s.qe[atomicAdd(&s.qcount[1], 1u)] = j;
+        const int2 *prs = s.pairs + o;
+        double sum;
+        if (kbn_stream_checked<STREAM_D>(nc, self_term<UNIF>(s, j, u, v), [&](int k) {
+                const int2 pr = prs[k];
+                return dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
+            }, sum))
+            delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, sum));
+        else
+            s.qe[atomicAdd(&s.qcount[1], 1u)] = j;
     }
     block_max_to(&s.maxd[s.slot], delta);
 }
@@ -536,7 +613,7 @@ __global__ void __launch_bounds__(128) k_vertex_med_sum(Sweep s)
         const int i = s.qv[q];
         const long long b = s.row_off[i];
         const int deg = (int)(s.row_off[i + 1] - b);
-        s.vd[i] = dsqrt(kbn_merge_buf(s.skey + (b - s.sbase), deg, four_nw(s, i)));
+        s.vd[i] = dsqrt(kbn_merge_stream(s.skey + (b - s.sbase), deg, four_nw(s, i)));
     }
 }
 
@@ -551,8 +628,8 @@ __global__ void __launch_bounds__(128) k_edge_med_sum(Sweep s)
         const long long o = s.ioff[j];
         const int nc = (int)(s.ioff[j + 1] - o);
         const int u = s.eu[j], v = s.ev[j];
-        delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_merge_buf(s.tkey + (o - s.tbase), nc,
-                                                                       self_term<UNIF>(s, j, u, v))));
+        delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_merge_stream(s.tkey + (o - s.tbase), nc,
+                                                                          self_term<UNIF>(s, j, u, v))));
     }
     block_max_to(&s.maxd[s.slot], delta);
 }
@@ -645,27 +722,45 @@ __global__ void __launch_bounds__(512) k_edge_block(Sweep s, int begin, int end,
     if (SUM_HERE) block_max_to(&s.maxd[s.slot], delta);
 }
 
-// one thread per block item: the sequential sum of its sorted slot
+// The sequential sums of the block items' sorted slots, in 32-thread
+// blocks.  A chain of thousands of terms is bound by the latency of its
+// additions, so each BBIG item (the longest) gets a block of its own, one
+// lane working, and the block scheduler spreads those over the SMs; the
+// BBLOCK items follow, one lane each.  Both ranges are ordered longest first.
 template <bool UNIF>
-__global__ void __launch_bounds__(128) k_vertex_block_sum(Sweep s, int begin, int end)
+__global__ void __launch_bounds__(32) k_vertex_block_sum(Sweep s, int big0, int nbig, int blk0, int nblk)
 {
     if (skipped(s)) return;
-    const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= end) return;
+    int i;
+    if ((int)blockIdx.x < nbig) {
+        if (threadIdx.x) return;
+        i = big0 + (int)blockIdx.x;
+    } else {
+        const int t = ((int)blockIdx.x - nbig) * 32 + (int)threadIdx.x;
+        if (t >= nblk) return;
+        i = blk0 + t;
+    }
     const int deg = (int)(s.row_off[i + 1] - s.row_off[i]);
-    s.vd[i] = dsqrt(kbn_merge_buf(s.bkey_v + s.bofs_v[i - s.bv0], deg, four_nw(s, i)));
+    s.vd[i] = dsqrt(kbn_merge_stream(s.bkey_v + s.bofs_v[i - s.bv0], deg, four_nw(s, i)));
 }
 
 template <bool UNIF>
-__global__ void __launch_bounds__(128) k_edge_block_sum(Sweep s, int begin, int end)
+__global__ void __launch_bounds__(32) k_edge_block_sum(Sweep s, int big0, int nbig, int blk0, int nblk)
 {
     if (skipped(s)) return;
-    const int j = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    int j = -1;
+    if ((int)blockIdx.x < nbig) {
+        if (threadIdx.x == 0) j = big0 + (int)blockIdx.x;
+    } else {
+        const int t = ((int)blockIdx.x - nbig) * 32 + (int)threadIdx.x;
+        if (t < nblk) j = blk0 + t;
+    }
     double delta = 0.0;
-    if (j < end) {
+    if (j >= 0) {
         const int u = s.eu[j], v = s.ev[j];
         const int nc = (int)(s.ioff[j + 1] - s.ioff[j]);
-        delta = finish_edge<UNIF>(s, j, u, v, kbn_merge_buf(s.bkey_e + s.bofs_e[j - s.be0], nc, self_term<UNIF>(s, j, u, v)));
+        delta = finish_edge<UNIF>(s, j, u, v, kbn_merge_stream(s.bkey_e + s.bofs_e[j - s.be0], nc,
+                                                               self_term<UNIF>(s, j, u, v)));
     }
     block_max_to(&s.maxd[s.slot], delta);
 }
@@ -702,18 +797,14 @@ inline size_t med_smem_edge() { return (size_t)(MED_THR / 32) * MED_CAP * (8 + 8
 template <bool UNIF>
 Status set_sweep_attributes(int block_cap, int vblock_cap)
 {
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_block<UNIF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        vblock_cap * 12));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_block<UNIF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        block_cap * 16));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_block<UNIF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        BIG_CAP * 12));
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_block<UNIF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        BIG_CAP * 16));
     DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_med_sort<UNIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)med_smem_vertex()));
     DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_med_sort<UNIF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)med_smem_edge()));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_vertex_block<UNIF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        std::max(BIG_CAP, vblock_cap) * 12));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_edge_block<UNIF, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        std::max(BIG_CAP, block_cap) * 16));
     return Status::Ok();
 }
 
@@ -724,11 +815,11 @@ void launch_blocks(const Sweep &s, const Bins &b, const LaunchCfg &c)
 {
     if (b.has(BBIG)) {
         if (EDGE)
-            count_launch(), k_edge_block<UNIF, true><<<grid_for(b.count(BBIG), 1, c.sms), 512, (size_t)c.block_cap * 16,
-                                                 c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.block_cap);
+            count_launch(), k_edge_block<UNIF, false><<<grid_for(b.count(BBIG), 1, c.sms), 512, (size_t)c.block_cap * 16,
+                                                  c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.block_cap);
         else
-            count_launch(), k_vertex_block<UNIF, true><<<grid_for(b.count(BBIG), 1, c.sms), 512, (size_t)c.vblock_cap * 12,
-                                                   c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.vblock_cap);
+            count_launch(), k_vertex_block<UNIF, false><<<grid_for(b.count(BBIG), 1, c.sms), 512, (size_t)c.vblock_cap * 12,
+                                                    c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.vblock_cap);
     }
     if (b.has(BBLOCK)) {
         if (EDGE)
@@ -738,11 +829,13 @@ void launch_blocks(const Sweep &s, const Bins &b, const LaunchCfg &c)
             count_launch(), k_vertex_block<UNIF, false><<<grid_for(b.count(BBLOCK), 1, 4 * c.sms), 512, (size_t)BIG_CAP * 12,
                                                    c.side>>>(s, b.start[BBLOCK], b.start[BBLOCK + 1], BIG_CAP);
     }
-    const int n = b.count(BBLOCK);                       // BBIG items are summed in their block
-    if (n > 0) {
-        const int first = b.start[BBLOCK];
-        if (EDGE) count_launch(), k_edge_block_sum<UNIF><<<grid_for(n, THR, INT_MAX), THR, 0, c.side>>>(s, first, first + n);
-        else count_launch(), k_vertex_block_sum<UNIF><<<grid_for(n, THR, INT_MAX), THR, 0, c.side>>>(s, first, first + n);
+    const int nblk = b.count(BBLOCK), nbig = b.count(BBIG);
+    if (nblk + nbig > 0) {
+        const unsigned g = (unsigned)(nbig + (nblk + 31) / 32);
+        if (EDGE)
+            count_launch(), k_edge_block_sum<UNIF><<<g, 32, 0, c.side>>>(s, b.start[BBIG], nbig, b.start[BBLOCK], nblk);
+        else
+            count_launch(), k_vertex_block_sum<UNIF><<<g, 32, 0, c.side>>>(s, b.start[BBIG], nbig, b.start[BBLOCK], nblk);
     }
 }
 
