@@ -123,6 +123,8 @@ struct Prep {
     double *ms_host = nullptr;         // multiset matrix (caller owns after return)
     std::vector<long long> values_host;  // per-subgraph path: values collected on the host
     std::vector<long long> hist;       // flat [bits, count]
+    int64_t *hist_mal = nullptr;       // ... or already in a malloc'd array
+    long long hist_mal_len = 0;
     unsigned long long sweeps = 0, edge_iters = 0, fits = 0;
 };
 
@@ -619,9 +621,14 @@ Status collect_batched(BatchPlan &P, const Ctx &en)
         ps[(size_t)i]->fits = st_i[ST_FITS];
     }
     if (P.need_hist) {
-        std::vector<std::vector<long long>> out;
-        DRESS_TRY(histogram_download(P.hist, out, st));
-        for (int i = 0; i < nreq; ++i) ps[(size_t)i]->hist = std::move(out[(size_t)i]);
+        std::vector<int64_t *> outs;
+        std::vector<long long> lens;
+        DRESS_TRY(histogram_fetch(P.hist, outs, lens, &engine().pinned, st, en.num_sms));
+        for (int i = 0; i < nreq; ++i) {
+            std::free(ps[(size_t)i]->hist_mal);
+            ps[(size_t)i]->hist_mal = outs[(size_t)i];
+            ps[(size_t)i]->hist_mal_len = lens[(size_t)i];
+        }
     }
     if (P.ms_total > 0) {
         size_t o = 0;
@@ -762,7 +769,12 @@ Status finish(Prep &p)
     r->fits = (int64_t)p.fits;
     r->hist_flat = nullptr;
     r->hist_len = 0;
-    if (r->want_histogram && !p.hist.empty()) {
+    if (r->want_histogram && p.hist_mal) {          // hand over the fetched array
+        r->hist_flat = p.hist_mal;
+        r->hist_len = (int)p.hist_mal_len;
+        p.hist_mal = nullptr;
+        p.hist_mal_len = 0;
+    } else if (r->want_histogram && !p.hist.empty()) {
         r->hist_flat = (int64_t *)std::malloc(p.hist.size() * sizeof(int64_t));
         if (!r->hist_flat) return Status::Err(DRESSX_ENOMEM, "host allocation of the histogram failed");
         std::memcpy(r->hist_flat, p.hist.data(), p.hist.size() * sizeof(int64_t));
@@ -843,6 +855,8 @@ Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const C
             if (!s.ok()) { p.r->status = s.code; if (first.ok()) first = s; }
         }
         if (p.ms_host) { std::free(p.ms_host); p.ms_host = nullptr; }
+        std::free(p.hist_mal);
+        p.hist_mal = nullptr;
     }
     if (edge_sweeps)
         for (int i = 0; i < n; ++i) edge_sweeps[i] = (int64_t)ps[(size_t)i].edge_iters;
@@ -1152,7 +1166,10 @@ void dressx_batch_destroy(dressx_batch_t *b)
     if (!b) return;
     Engine &en = engine();
     std::lock_guard<std::mutex> lk(en.mu);
-    for (auto &p : b->preps) std::free(p.ms_host);
+    for (auto &p : b->preps) {
+        std::free(p.ms_host);
+        std::free(p.hist_mal);
+    }
     delete b;
     cudaStreamSynchronize(en.ctx.st);
 }

@@ -151,6 +151,12 @@ int dressx_last_fit_stats(dressx_fit_stats_t *out)
     out->sweeps = g_last_stats.sweeps;
     out->setup_ms = g_last_stats.setup_ms;
     out->iterate_ms = g_last_stats.iterate_ms;
+    for (int b = 0; b < 8; ++b) {
+        out->vertex_bin_items[b] = g_last_stats.vbin_items[b];
+        out->vertex_bin_terms[b] = g_last_stats.vbin_terms[b];
+        out->edge_bin_items[b] = g_last_stats.ebin_items[b];
+        out->edge_bin_terms[b] = g_last_stats.ebin_terms[b];
+    }
     return DRESSX_OK;
 }
 

@@ -149,6 +149,7 @@ struct FitStats {
     long long T = 0;            // common-neighbour terms per sweep
     int sweeps = 0;             // sweeps executed
     double setup_ms = 0, iterate_ms = 0;
+    long long vbin_items[8] = {}, vbin_terms[8] = {}, ebin_items[8] = {}, ebin_terms[8] = {};
 };
 Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon,
                  int *iterations, double *delta, FitStats *stats, const Ctx &ctx);

@@ -217,6 +217,18 @@ __global__ void k_bin_count(int n, const int *len, int *bin_cnt)
         if (sc[f]) atomicAdd(&bin_cnt[f], sc[f]);
 }
 
+// stored terms per coarse bin
+__global__ void k_bin_terms(int n, const int *len, unsigned long long *terms)
+{
+    __shared__ unsigned long long sc[NB];
+    if (threadIdx.x < NB) sc[threadIdx.x] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(&sc[bin_of((long long)len[i])], (unsigned long long)len[i]);
+    __syncthreads();
+    if (threadIdx.x < NB && sc[threadIdx.x]) atomicAdd(&terms[threadIdx.x], sc[threadIdx.x]);
+}
+
 // Scatter items to their fine keys' ranges; lanes of a warp that share a key
 // take consecutive slots (one atomic per group), which keeps neighbouring
 // items neighbours.
@@ -460,6 +472,13 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     const int vg = (int)grid_for(N, 256, 32 * sms);
     count_launch(), k_bin_count<<<vg, 256, 0, st>>>(N, d_deg.get(), d_bc.get());
     count_launch(), k_bin_count<<<eg, 256, 0, st>>>(E, d_cnt.get(), d_bc.get() + NF);
+    DevBuf<unsigned long long> d_bterms;
+    DRESS_TRY(d_bterms.alloc(2 * NB, st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_bterms.get(), 0, 2 * NB * sizeof(unsigned long long), st));
+    count_launch(), k_bin_terms<<<vg, 256, 0, st>>>(N, d_deg.get(), d_bterms.get());
+    count_launch(), k_bin_terms<<<eg, 256, 0, st>>>(E, d_cnt.get(), d_bterms.get() + NB);
+    unsigned long long bterms[2 * NB];
+    DRESS_CUDA_TRY(counted_memcpy(bterms, d_bterms.get(), sizeof(bterms), cudaMemcpyDeviceToHost, st));
     std::vector<int> bc(2 * NF);
     DRESS_CUDA_TRY(counted_memcpy(bc.data(), d_bc.get(), 2 * NF * sizeof(int), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
@@ -708,6 +727,12 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     if (iterations) *iterations = conv >= 0 ? conv : max_iterations;
     if (delta) *delta = last_delta;
     if (stats) {
+        for (int b = 0; b < NB && b < 8; ++b) {
+            stats->vbin_items[b] = vb.count(b);
+            stats->ebin_items[b] = eb.count(b);
+            stats->vbin_terms[b] = (long long)bterms[b];
+            stats->ebin_terms[b] = (long long)bterms[NB + b];
+        }
         stats->T = T;
         stats->sweeps = last + 1;
         stats->setup_ms = setup_ms;

@@ -11,7 +11,10 @@
 // reference's map.  A pass in which every segment has a single digit value
 // moves nothing and is skipped.
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "engine.h"
@@ -299,6 +302,87 @@ Status histogram_device(unsigned long long *keys, unsigned long long *alt, const
         R, d_run_start.get(), d_run_bits.get(), res.run_seg.get(), d_seg_end.get(), res.pairs.get());
     DRESS_CUDA_TRY(cudaGetLastError());
     res.R = R;
+    return Status::Ok();
+}
+
+// end (one past the last run) of every segment that has runs
+__global__ void k_seg_ends(long long R, const int *run_seg, long long *seg_end)
+{
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < R;
+         r += (long long)gridDim.x * blockDim.x)
+        if (r + 1 == R || run_seg[r + 1] != run_seg[r]) seg_end[run_seg[r]] = r + 1;
+}
+
+Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
+                       cudaStream_t st, int sms)
+{
+    const int nseg = res.nseg;
+    outs.assign((size_t)nseg, nullptr);
+    lens.assign((size_t)nseg, 0);
+    const long long R = res.R;
+    if (R == 0) return Status::Ok();
+    DevBuf<long long> d_end;
+    DRESS_TRY(d_end.alloc((size_t)nseg, st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_end.get(), 0, (size_t)nseg * sizeof(long long), st));
+    count_launch(), k_seg_ends<<<(unsigned)((R + 255) / 256 < 16 * sms ? (R + 255) / 256 : 16 * sms), 256, 0, st>>>(
+        R, res.run_seg.get(), d_end.get());
+    std::vector<long long> end((size_t)nseg);
+    DRESS_CUDA_TRY(counted_memcpy(end.data(), d_end.get(), (size_t)nseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    const size_t bytes = 2 * (size_t)R * sizeof(long long);
+    long long *host = nullptr;
+    std::vector<long long> pageable;
+    if (stage && stage->reserve(bytes).ok()) {
+        host = (long long *)stage->ptr();
+    } else {
+        pageable.resize(2 * (size_t)R);
+        host = pageable.data();
+    }
+    DRESS_CUDA_TRY(counted_memcpy(host, res.pairs.get(), bytes, cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    // runs are grouped by segment in segment order: a segment starts where the
+    // last non-empty one before it ended
+    std::vector<long long> first((size_t)nseg, 0);
+    long long prev = 0;
+    for (int sg = 0; sg < nseg; ++sg) {
+        if (end[(size_t)sg] > 0) {
+            first[(size_t)sg] = prev;
+            lens[(size_t)sg] = 2 * (end[(size_t)sg] - prev);
+            prev = end[(size_t)sg];
+        }
+    }
+    for (int sg = 0; sg < nseg; ++sg)
+        if (lens[(size_t)sg] > 0) {
+            outs[(size_t)sg] = (int64_t *)std::malloc((size_t)lens[(size_t)sg] * sizeof(int64_t));
+            if (!outs[(size_t)sg]) {
+                for (auto &o : outs) std::free(o);
+                outs.assign((size_t)nseg, nullptr);
+                return Status::Err(DRESSX_ENOMEM, "host allocation of the histograms failed");
+            }
+        }
+    // copy out, several threads for large results
+    auto copy_range = [&](int a, int b) {
+        for (int sg = a; sg < b; ++sg)
+            if (lens[(size_t)sg] > 0)
+                std::memcpy(outs[(size_t)sg], host + 2 * first[(size_t)sg], (size_t)lens[(size_t)sg] * sizeof(int64_t));
+    };
+    const int nthr = bytes > (64u << 20) ? 8 : 1;
+    if (nthr == 1 || nseg < 2) {
+        copy_range(0, nseg);
+    } else {
+        // split by bytes so the threads copy about the same amount
+        std::vector<int> cut(1, 0);
+        const long long per = (2 * R + nthr - 1) / nthr;
+        long long acc = 0;
+        for (int sg = 0; sg < nseg; ++sg) {
+            acc += lens[(size_t)sg];
+            if (acc >= per * (long long)cut.size() && (int)cut.size() < nthr) cut.push_back(sg + 1);
+        }
+        cut.push_back(nseg);
+        std::vector<std::thread> th;
+        for (size_t t = 0; t + 1 < cut.size(); ++t)
+            if (cut[t + 1] > cut[t]) th.emplace_back(copy_range, cut[t], cut[t + 1]);
+        for (auto &t : th) t.join();
+    }
     return Status::Ok();
 }
 

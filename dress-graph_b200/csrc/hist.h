@@ -19,6 +19,11 @@ struct HistResult {
 Status histogram_device(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
                         const std::vector<long long> &len, HistResult &res, cudaStream_t st, int sms);
 Status histogram_download(HistResult &res, std::vector<std::vector<long long>> &out, cudaStream_t st);
+// Same results straight into malloc'd per-segment arrays (outs[s], lens[s]
+// int64 entries; NULL and 0 for an empty segment; the caller frees them),
+// through the pinned staging buffer when one is given.
+Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
+                       cudaStream_t st, int sms);
 
 // Sorts each segment [begin[s], begin[s]+len[s]) of `keys` (raw double bits)
 // and returns, per segment, the flat [value_bits, count, ...] list ascending

@@ -8,6 +8,7 @@ Same entry points, argument names, defaults and result fields as
 many graphs' histograms in one persistent launch.
 """
 import ctypes
+import weakref
 from dataclasses import dataclass, field
 from typing import List, Optional, Tuple
 
@@ -55,6 +56,20 @@ def _malloc_copy(arr, ctype):
     if arr.nbytes:
         ctypes.memmove(raw, arr.ctypes.data, arr.nbytes)
     return ctypes.cast(raw, ctypes.POINTER(ctype))
+
+
+def _take_i64(ptr, n):
+    """A malloc'd int64 array from the library as numpy, without a copy; the
+    memory is released with dressx_free once no array refers to it."""
+    if not ptr:
+        return np.zeros(0, dtype=np.int64)
+    addr = ctypes.cast(ptr, ctypes.c_void_p).value
+    if n <= 0:
+        lib().dressx_free(addr)
+        return np.zeros(0, dtype=np.int64)
+    buf = (ctypes.c_int64 * int(n)).from_address(addr)
+    weakref.finalize(buf, lib().dressx_free, addr)
+    return np.frombuffer(buf, dtype=np.int64)
 
 
 def _arr(ptr, n, dtype):
@@ -156,7 +171,9 @@ def fit_graph(g: Graph, max_iterations=100, epsilon=1e-6):
 def last_fit_stats():
     st = _abi.FitStats()
     lib().dressx_last_fit_stats(ctypes.byref(st))
-    return dict(common_terms=st.common_terms, sweeps=st.sweeps, setup_ms=st.setup_ms, iterate_ms=st.iterate_ms)
+    return dict(common_terms=st.common_terms, sweeps=st.sweeps, setup_ms=st.setup_ms, iterate_ms=st.iterate_ms,
+                vertex_bins=list(zip(st.vertex_bin_items, st.vertex_bin_terms)),
+                edge_bins=list(zip(st.edge_bin_items, st.edge_bin_terms)))
 
 
 def dress_cuda(N, E, U, V, W=None, NW=None, variant=UNDIRECTED, precompute_intercepts=0,
@@ -222,9 +239,8 @@ def hist_requests(graphs, kind, k, max_iterations=100, epsilon=1e-6, n_samples=0
     out = []
     for i, g in enumerate(graphs):
         r = reqs[i]
-        flat = _arr(r.hist_flat, r.hist_len, np.int64)
-        if r.hist_flat:
-            lib().dressx_free(ctypes.cast(r.hist_flat, ctypes.c_void_p))
+        flat = _take_i64(r.hist_flat, r.hist_len)
+        r.hist_flat = None
         ms = None
         if r.multisets:
             ms = _arr(r.multisets, r.num_subgraphs * g.E, np.float64).reshape(r.num_subgraphs, g.E)
@@ -320,7 +336,8 @@ class Batch:
         out = []
         for i in range(len(self.graphs)):
             r = self.reqs[i]
-            out.append(_arr(r.hist_flat, r.hist_len, np.int64))
+            out.append(_take_i64(r.hist_flat, r.hist_len))
+            r.hist_flat = None                       # the array owns it now
         return out
 
     def stats(self):
@@ -416,10 +433,8 @@ class Ticket:
         if r.kind == FIT:
             out.update(iterations=r.iterations, delta=r.delta)
         else:
-            flat = _arr(r.hist_flat, r.hist_len, np.int64)
-            if r.hist_flat:
-                lib().dressx_free(ctypes.cast(r.hist_flat, ctypes.c_void_p))
-                r.hist_flat = None
+            flat = _take_i64(r.hist_flat, r.hist_len)
+            r.hist_flat = None
             out.update(hist_flat=flat, num_subgraphs=r.num_subgraphs)
         self._result = out
         return out

@@ -59,7 +59,9 @@ class Config(ctypes.Structure):
 
 class FitStats(ctypes.Structure):
     _fields_ = [("common_terms", ctypes.c_int64), ("sweeps", ctypes.c_int),
-                ("setup_ms", ctypes.c_double), ("iterate_ms", ctypes.c_double)]
+                ("setup_ms", ctypes.c_double), ("iterate_ms", ctypes.c_double),
+                ("vertex_bin_items", ctypes.c_int64 * 8), ("vertex_bin_terms", ctypes.c_int64 * 8),
+                ("edge_bin_items", ctypes.c_int64 * 8), ("edge_bin_terms", ctypes.c_int64 * 8)]
 
 
 class ServerConfig(ctypes.Structure):

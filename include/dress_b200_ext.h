@@ -57,6 +57,10 @@ typedef struct dressx_fit_stats_t {
     int     sweeps;            /* sweeps executed                          */
     double  setup_ms;          /* upload + intercepts + binning            */
     double  iterate_ms;        /* all sweeps, device time (CUDA events)    */
+    /* items and stored terms per size bin (0, <=2, <=4, <=8, <=16, <=512,
+     * <=4096, more terms), vertices (row slots) and edges (common pairs) */
+    int64_t vertex_bin_items[8], vertex_bin_terms[8];
+    int64_t edge_bin_items[8], edge_bin_terms[8];
 } dressx_fit_stats_t;
 int dressx_last_fit_stats(dressx_fit_stats_t *out);
 
