@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--graphs", type=int, default=2000)
     ap.add_argument("--no-single-fit", action="store_true", help="skip the 28M-edge single fit")
     ap.add_argument("--single-fit-edges", type=int, default=28_000_000)
+    ap.add_argument("--single-fit-only", action="store_true",
+                    help="run only the single large fit and print its JSON object (profiling runs)")
+    ap.add_argument("--single-fit-variants", default="weighted,unweighted")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving stream")
     ap.add_argument("--no-k2", action="store_true", help="skip the Delta^2 / Nabla^1 workload")
@@ -308,7 +311,10 @@ def bench_single_fit(args, torch):
     E = len(U)
     out = {"workload": f"Chung-Lu power law, N={n}, E={E}, gamma 2.3, max degree 20000, epsilon 1e-6"}
     peak, peak_kind = peaks()
+    variants = [v for v in args.single_fit_variants.split(",") if v]
     for label, W in (("weighted", graphs.uniform_weights(E, seed=7)), ("unweighted", None)):
+        if label not in variants:
+            continue
         g = db.Graph(n, U, V, W)
         S = int(g.ptr.contents.adj_offset[n])
         db.counters(reset=True)
@@ -657,6 +663,9 @@ def main():
     torch.cuda.set_device(local)
     import dress_b200 as db
     db.configure(device=local)
+    if args.single_fit_only:
+        print(json.dumps({"single_fit": bench_single_fit(args, torch)}), flush=True)
+        return
     clocks = Clocks(local)
     head = bench_delta1(args, rank, world, pg, torch, clocks)
     single = None
