@@ -216,14 +216,21 @@ __global__ void k_run_pairs(long long R, const long long *run_start, const unsig
     }
 }
 
-}  // namespace
+// Tiles of the segments, uploaded, and the keys sorted (order-preserving
+// image) within every segment; `out` is the buffer holding the result.
+struct SortPlan {
+    DevBuf<Tile> tiles;
+    DevBuf<long long> seg_begin, seg_end;
+    int nt = 0, nseg = 0;
+    unsigned long long *out = nullptr;
+};
 
-Status histogram_device(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
-                        const std::vector<long long> &len, HistResult &res, cudaStream_t st, int sms)
+Status sort_segments(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
+                     const std::vector<long long> &len, SortPlan &sp, cudaStream_t st, int sms)
 {
     const int nseg = (int)begin.size();
-    res.nseg = nseg;
-    res.R = 0;
+    sp.nseg = nseg;
+    sp.out = keys;
     std::vector<Tile> tiles;
     std::vector<int> seg_tile0((size_t)nseg + 1, 0);
     std::vector<long long> seg_end((size_t)nseg);
@@ -240,26 +247,25 @@ Status histogram_device(unsigned long long *keys, unsigned long long *alt, const
         }
     }
     seg_tile0[(size_t)nseg] = (int)tiles.size();
+    sp.nt = (int)tiles.size();
     if (total == 0) return Status::Ok();
-    const int nt = (int)tiles.size();
+    const int nt = sp.nt;
 
-    DevBuf<Tile> d_tiles;
     DevBuf<int> d_seg_tile0, d_counts, d_moves;
-    DevBuf<long long> d_seg_begin, d_seg_end, d_offs, d_tile_heads, d_tile_base, d_scan_tmp, d_run_start;
-    DevBuf<unsigned long long> d_run_bits;
-    DRESS_TRY(d_tiles.alloc((size_t)nt, st));
+    DevBuf<long long> d_offs;
+    DRESS_TRY(sp.tiles.alloc((size_t)nt, st));
     DRESS_TRY(d_seg_tile0.alloc((size_t)nseg + 1, st));
-    DRESS_TRY(d_seg_begin.alloc((size_t)nseg, st));
-    DRESS_TRY(d_seg_end.alloc((size_t)nseg, st));
+    DRESS_TRY(sp.seg_begin.alloc((size_t)nseg, st));
+    DRESS_TRY(sp.seg_end.alloc((size_t)nseg, st));
     DRESS_TRY(d_counts.alloc((size_t)nt * RADIX, st));
     DRESS_TRY(d_offs.alloc((size_t)nt * RADIX, st));
     DRESS_TRY(d_moves.alloc(1, st));
-    DRESS_CUDA_TRY(counted_memcpy(d_tiles.get(), tiles.data(), (size_t)nt * sizeof(Tile), cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(counted_memcpy(sp.tiles.get(), tiles.data(), (size_t)nt * sizeof(Tile), cudaMemcpyHostToDevice, st));
     DRESS_CUDA_TRY(counted_memcpy(d_seg_tile0.get(), seg_tile0.data(), ((size_t)nseg + 1) * sizeof(int),
                                    cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(counted_memcpy(d_seg_begin.get(), begin.data(), (size_t)nseg * sizeof(long long),
+    DRESS_CUDA_TRY(counted_memcpy(sp.seg_begin.get(), begin.data(), (size_t)nseg * sizeof(long long),
                                    cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(counted_memcpy(d_seg_end.get(), seg_end.data(), (size_t)nseg * sizeof(long long),
+    DRESS_CUDA_TRY(counted_memcpy(sp.seg_end.get(), seg_end.data(), (size_t)nseg * sizeof(long long),
                                    cudaMemcpyHostToDevice, st));
 
     // order-preserving image of the doubles over the used span
@@ -268,26 +274,56 @@ Status histogram_device(unsigned long long *keys, unsigned long long *alt, const
     unsigned long long *a = keys, *b = alt;
     for (int pass = 0; pass < 8; ++pass) {
         int shift = 8 * pass;
-        count_launch(), k_tile_hist<<<nt, HT, 0, st>>>(d_tiles.get(), a, shift, d_counts.get());
+        count_launch(), k_tile_hist<<<nt, HT, 0, st>>>(sp.tiles.get(), a, shift, d_counts.get());
         DRESS_CUDA_TRY(cudaMemsetAsync(d_moves.get(), 0, sizeof(int), st));
-        count_launch(), k_seg_offsets<<<nseg, RADIX, 0, st>>>(d_seg_begin.get(), d_seg_tile0.get(), d_counts.get(), d_offs.get(),
-                                              d_moves.get());
+        count_launch(), k_seg_offsets<<<nseg, RADIX, 0, st>>>(sp.seg_begin.get(), d_seg_tile0.get(), d_counts.get(),
+                                                              d_offs.get(), d_moves.get());
         int moves = 0;
         DRESS_CUDA_TRY(counted_memcpy(&moves, d_moves.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         if (!moves) continue;
-        count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(d_tiles.get(), a, b, shift, d_offs.get());
+        count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(sp.tiles.get(), a, b, shift, d_offs.get());
         unsigned long long *t = a;
         a = b;
         b = t;
     }
     DRESS_CUDA_TRY(cudaGetLastError());
+    sp.out = a;
+    return Status::Ok();
+}
+
+}  // namespace
+
+Status segmented_sort(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
+                      const std::vector<long long> &len, unsigned long long **sorted, cudaStream_t st, int sms)
+{
+    SortPlan sp;
+    DRESS_TRY(sort_segments(keys, alt, begin, len, sp, st, sms));
+    *sorted = sp.out;
+    return Status::Ok();
+}
+
+Status histogram_device(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
+                        const std::vector<long long> &len, HistResult &res, cudaStream_t st, int sms)
+{
+    const int nseg = (int)begin.size();
+    res.nseg = nseg;
+    res.R = 0;
+    long long total = 0;
+    for (long long l : len) total += l;
+    if (total == 0) return Status::Ok();
+    SortPlan sp;
+    DRESS_TRY(sort_segments(keys, alt, begin, len, sp, st, sms));
+    const int nt = sp.nt;
+    unsigned long long *a = sp.out;
+    DevBuf<long long> d_tile_heads, d_tile_base, d_scan_tmp, d_run_start;
+    DevBuf<unsigned long long> d_run_bits;
 
     // run-length encode
     DRESS_TRY(d_tile_heads.alloc((size_t)nt, st));
     DRESS_TRY(d_tile_base.alloc((size_t)nt + 1, st));
     DRESS_TRY(d_scan_tmp.alloc(scan_tmp_elems(nt), st));
-    count_launch(), k_tile_heads<<<nt, HT, 0, st>>>(d_tiles.get(), d_seg_begin.get(), a, d_tile_heads.get());
+    count_launch(), k_tile_heads<<<nt, HT, 0, st>>>(sp.tiles.get(), sp.seg_begin.get(), a, d_tile_heads.get());
     DRESS_TRY(exclusive_scan_i64(d_tile_heads.get(), d_tile_base.get(), nt, d_scan_tmp.get(), st));
     long long R = 0;
     DRESS_CUDA_TRY(counted_memcpy(&R, d_tile_base.get() + nt, sizeof(R), cudaMemcpyDeviceToHost, st));
@@ -296,10 +332,10 @@ Status histogram_device(unsigned long long *keys, unsigned long long *alt, const
     DRESS_TRY(d_run_bits.alloc((size_t)R, st));
     DRESS_TRY(res.run_seg.alloc((size_t)R, st));
     DRESS_TRY(res.pairs.alloc(2 * (size_t)R, st));
-    count_launch(), k_tile_runs<<<nt, HT, 0, st>>>(d_tiles.get(), d_seg_begin.get(), a, d_tile_base.get(), d_run_start.get(),
+    count_launch(), k_tile_runs<<<nt, HT, 0, st>>>(sp.tiles.get(), sp.seg_begin.get(), a, d_tile_base.get(), d_run_start.get(),
                                    d_run_bits.get(), res.run_seg.get());
     count_launch(), k_run_pairs<<<(unsigned)((R + 255) / 256 < 64 * sms ? (R + 255) / 256 : 64 * sms), 256, 0, st>>>(
-        R, d_run_start.get(), d_run_bits.get(), res.run_seg.get(), d_seg_end.get(), res.pairs.get());
+        R, d_run_start.get(), d_run_bits.get(), res.run_seg.get(), sp.seg_end.get(), res.pairs.get());
     DRESS_CUDA_TRY(cudaGetLastError());
     res.R = R;
     return Status::Ok();

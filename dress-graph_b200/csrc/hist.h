@@ -25,6 +25,12 @@ Status histogram_download(HistResult &res, std::vector<std::vector<long long>> &
 Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
                        cudaStream_t st, int sms);
 
+// Sorts each segment [begin[s], begin[s]+len[s]) of `keys` (raw double bits,
+// replaced by their order-preserving image, see ordered_to_double) ascending;
+// *sorted is whichever of keys / alt holds the result.
+Status segmented_sort(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
+                      const std::vector<long long> &len, unsigned long long **sorted, cudaStream_t st, int sms);
+
 // Sorts each segment [begin[s], begin[s]+len[s]) of `keys` (raw double bits)
 // and returns, per segment, the flat [value_bits, count, ...] list ascending
 // by value with ==-equal values merged.  `alt` is scratch of the same size as

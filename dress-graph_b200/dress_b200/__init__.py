@@ -168,6 +168,31 @@ def fit_graph(g: Graph, max_iterations=100, epsilon=1e-6):
     return it.value, dl.value
 
 
+def get(g: Graph, u, v, max_iterations=100, epsilon=1e-6, edge_weight=1.0):
+    """Virtual-edge values for the vertex pairs (u[i], v[i]) of a fitted graph
+    (the reference's dress_get, many pairs in one call).  edge_weight is a
+    scalar or one weight per pair."""
+    u = np.ascontiguousarray(u, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.int32)
+    if u.shape != v.shape:
+        raise ValueError("u and v differ in length")
+    out = np.empty(u.size, dtype=np.float64)
+    ew = None
+    ew0 = 1.0
+    if np.ndim(edge_weight) == 0:
+        ew0 = float(edge_weight)
+    else:
+        ew = np.ascontiguousarray(edge_weight, dtype=np.float64)
+        if ew.shape != u.shape:
+            raise ValueError("one edge weight per pair")
+    ip = ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    _check(lib().dressx_get_batch(g.ptr, u.ctypes.data_as(ip), v.ctypes.data_as(ip), u.size, int(max_iterations),
+                                  float(epsilon), ew.ctypes.data_as(dp) if ew is not None else None, ew0,
+                                  out.ctypes.data_as(dp)))
+    return out
+
+
 def last_fit_stats():
     st = _abi.FitStats()
     lib().dressx_last_fit_stats(ctypes.byref(st))

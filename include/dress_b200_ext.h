@@ -163,6 +163,17 @@ int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, i
 int dressx_histogram_noalloc(const double *values, int64_t n, int64_t *pairs, int64_t *num_runs,
                              void *stream);
 
+/* Batched virtual-edge queries on a fitted graph: out[i] is what the
+ * reference's dress_get(g, u[i], v[i], max_iterations, epsilon, w) returns
+ * (libdress/include/dress/dress.h:105, libdress/src/dress.c:651-739) -- the
+ * stored value of an existing edge, else the pair's own fixed point with
+ * every other value frozen -- with w = edge_weights[i], or edge_weight when
+ * edge_weights is NULL.  u, v, edge_weights and out are host arrays of n
+ * entries; the graph's current edge and vertex values are used.  A vertex
+ * out of range fails the call with DRESSX_EINVAL. */
+int dressx_get_batch(p_dress_graph_t g, const int *u, const int *v, int64_t n, int max_iterations,
+                     double epsilon, const double *edge_weights, double edge_weight, double *out);
+
 /* Merge of histograms computed on disjoint shards of one request (e.g. the
  * strided slices offset = rank, stride = ranks of several GPUs or
  * processes): n flat [value_bits, count, ...] lists, each ascending by value,

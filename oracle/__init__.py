@@ -101,6 +101,9 @@ class CpuDress:
         for f in (self.delta_fn, self.nabla_fn):
             f.restype = ctypes.POINTER(ctypes.c_int64)
             f.argtypes = hist_args
+        self.get_fn = getattr(lib, p + "get")
+        self.get_fn.restype = ctypes.c_double
+        self.get_fn.argtypes = [PGraph, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double]
         self.lib = lib
         if kind == "reference":
             self.fit_omp = lib.dress_fit_omp
@@ -151,6 +154,18 @@ class CpuDress:
                    iterations=it.value, delta=dl.value)
         self.free_graph(g)
         return res
+
+    # -- virtual-edge queries -------------------------------------------------
+    def get_many(self, N, U, V, W, queries, max_iterations=100, epsilon=1e-6, edge_weight=1.0,
+                 NW=None, variant=UNDIRECTED, fit_iterations=100, fit_epsilon=1e-6):
+        """Fit the graph, then dress_get for every (u, v) in queries."""
+        g = self.build(N, U, V, W, NW, variant, 0)
+        it, dl = ctypes.c_int(-1), ctypes.c_double(-1.0)
+        self.fit_fn(g, int(fit_iterations), float(fit_epsilon), ctypes.byref(it), ctypes.byref(dl))
+        out = np.array([self.get_fn(g, int(u), int(v), int(max_iterations), float(epsilon), float(edge_weight))
+                        for u, v in queries], dtype=np.float64)
+        self.free_graph(g)
+        return out
 
     # -- Delta / Nabla --------------------------------------------------------
     def _hist(self, fn, N, U, V, W, NW, variant, k, max_iterations, epsilon,

@@ -624,4 +624,61 @@ int64_t *oracle_nabla_fit_flat(p_dress_graph_t g, int k, int iterations,
 }
 
 /* Frees memory that this library returned (histograms, multisets). */
+/* ------------------------------------------------------------------ */
+/* virtual-edge query (dress.c:651-739)                                  */
+/* ------------------------------------------------------------------ */
+
+/* An existing edge returns its value; otherwise the common-neighbour terms of
+ * the frozen state plus the self-loop constant are summed (sorted KBN) and
+ * the pair's own value is iterated with everything else held fixed. */
+double oracle_get(p_dress_graph_t g, int u, int v, int max_iterations, double epsilon, double edge_weight)
+{
+    int lo = g->adj_offset[u], hi = g->adj_offset[u + 1] - 1;
+    while (lo <= hi) {
+        int mid = lo + (hi - lo) / 2;
+        int nb = g->adj_target[mid];
+        if (nb == v) return g->edge_dress[g->adj_edge_idx[mid]];
+        if (nb < v) lo = mid + 1;
+        else hi = mid - 1;
+    }
+    int du = g->adj_offset[u + 1] - g->adj_offset[u];
+    int dv = g->adj_offset[v + 1] - g->adj_offset[v];
+    double *t = (double *)malloc(((du < dv ? du : dv) + 1) * sizeof(double));
+    int n = 0;
+    int iu = g->adj_offset[u], iu_end = g->adj_offset[u + 1];
+    int iv = g->adj_offset[v], iv_end = g->adj_offset[v + 1];
+    while (iu < iu_end && iv < iv_end) {
+        int x = g->adj_target[iu], y = g->adj_target[iv];
+        if (x == y) {
+            int eu = g->adj_edge_idx[iu], ev = g->adj_edge_idx[iv];
+            t[n++] = g->edge_weight[eu] * g->edge_dress[eu] + g->edge_weight[ev] * g->edge_dress[ev];
+        }
+        iu += (x <= y);
+        iv += (x >= y);
+    }
+    int fwd = g->variant == DRESS_VARIANT_FORWARD || g->variant == DRESS_VARIANT_BACKWARD;
+    double nwu = g->NW ? g->NW[u] : 1.0, nwv = g->NW ? g->NW[v] : 1.0;
+    t[n++] = fwd ? 4.0 * nwu : 4.0 * nwu + 4.0 * nwv;
+    double A = oracle_kbn_sorted_sum(t, n);
+    free(t);
+    double cf = fwd ? 1.0 : 2.0;
+    double cw = g->variant == DRESS_VARIANT_UNDIRECTED ? 2.0 * edge_weight : edge_weight;
+    double du2 = g->vertex_dress[u] * g->vertex_dress[u];
+    double dv2 = g->vertex_dress[v] * g->vertex_dress[v];
+    if (du2 <= 0.0 || dv2 <= 0.0) return 0.0;
+    double d = 1.0;
+    for (int it = 0; it < max_iterations; ++it) {
+        double wd = cw * d;
+        double den = sqrt(du2 + wd) * sqrt(dv2 + wd);
+        if (den <= 0.0) return 0.0;
+        double nx = (A + cf * wd) / den;
+        if (fabs(nx - d) <= epsilon) {
+            d = nx;
+            break;
+        }
+        d = nx;
+    }
+    return d;
+}
+
 void oracle_free(void *p) { free(p); }

@@ -170,3 +170,44 @@ def test_reference_c_tests_through_redirect():
     out = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout[-3000:] + out.stderr[-2000:]
     assert " 0 failed" in out.stdout
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_virtual_edge_queries_match_oracle(oracle_port, variant):
+    """dressx_get_batch against the oracle's dress_get (pinned to the
+    reference): existing edges, non-edges with few and with many common
+    neighbours (register and sorted-slot paths), per-pair weights."""
+    rng = np.random.default_rng(7 + variant)
+    n, U, V = graphs.chung_lu(400, 3000, 2.3, 150, seed=11)
+    W = graphs.uniform_weights(len(U), seed=5)
+    NW = rng.uniform(0.5, 2.0, n)
+    deg = np.bincount(np.concatenate([U, V]), minlength=n)
+    hubs = np.argsort(-deg)[:12]
+    q = [(int(a), int(b)) for a, b in rng.integers(0, n, (600, 2))]
+    q += [(int(a), int(b)) for a in hubs for b in hubs if a != b]          # many common neighbours
+    q += [(int(U[i]), int(V[i])) for i in range(0, len(U), 37)]           # existing edges
+    qu = np.array([a for a, _ in q], np.int32)
+    qv = np.array([b for _, b in q], np.int32)
+    with db.Graph(n, U, V, W, NW, variant) as g:
+        db.fit_graph(g, 100, 1e-6)
+        got = db.get(g, qu, qv, 100, 1e-6, 0.8)
+        ews = rng.uniform(0.5, 2.0, len(q))
+        got_w = db.get(g, qu, qv, 50, 1e-9, ews)
+    ref = oracle_port.get_many(n, U, V, W, q, NW=NW, variant=variant, edge_weight=0.8)
+    np.testing.assert_array_equal(bits(got), bits(ref))
+    gb = oracle_port.build(n, U, V, W, NW, variant, 0)
+    it, dl = ctypes.c_int(), ctypes.c_double()
+    oracle_port.fit_fn(gb, 100, 1e-6, ctypes.byref(it), ctypes.byref(dl))
+    ref_w = np.array([oracle_port.get_fn(gb, a, b, 50, 1e-9, float(w)) for (a, b), w in zip(q, ews)])
+    oracle_port.free_graph(gb)
+    np.testing.assert_array_equal(bits(got_w), bits(ref_w))
+    assert max(int(deg[a]) for a in hubs) > 40
+
+
+def test_virtual_edge_query_rejects_bad_vertices():
+    n, U, V = graphs.erdos_renyi(50, 100, seed=2)
+    with db.Graph(n, U, V) as g:
+        db.fit_graph(g, 10, 1e-6)
+        with pytest.raises(db.DressError) as e:
+            db.get(g, [0, 60], [1, 2])
+        assert e.value.code == 1

@@ -147,3 +147,20 @@ def test_oracle_vs_reference_hist_random(oracle_port, oracle_ref):
                 np.testing.assert_array_equal(a["hist"], b["hist"])
                 assert a["num"] == b["num"]
                 np.testing.assert_array_equal(bits(a["multisets"]), bits(b["multisets"]))
+
+
+def test_virtual_edge_query_matches_reference(oracle_port, oracle_ref):
+    """dress_get (libdress/src/dress.c:651-739): existing edges, virtual
+    edges with and without common neighbours, every variant, weights."""
+    from dress_b200 import graphs
+    rng = np.random.default_rng(4)
+    n, U, V = graphs.chung_lu(300, 1500, 2.3, 60, seed=9)
+    W = graphs.uniform_weights(len(U), seed=3)
+    NW = rng.uniform(0.5, 2.0, n)
+    q = [(int(a), int(b)) for a, b in rng.integers(0, n, (400, 2)) if a != b]
+    q += [(int(U[i]), int(V[i])) for i in range(0, len(U), 50)]
+    for variant in range(4):
+        for w, nw, ew in ((None, None, 1.0), (W, NW, 0.7)):
+            a = oracle_port.get_many(n, U, V, w, q, NW=nw, variant=variant, edge_weight=ew)
+            b = oracle_ref.get_many(n, U, V, w, q, NW=nw, variant=variant, edge_weight=ew)
+            np.testing.assert_array_equal(a.view(np.int64), b.view(np.int64))
