@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(RADIX) k_seg_offsets(const long long *seg_begi
 // of the round) + (same digit in earlier rounds of the tile)
 __global__ void __launch_bounds__(HT) k_tile_scatter(const Tile *tiles, const unsigned long long *src,
                                                      unsigned long long *dst, int shift,
-                                                     const long long *offs)
+                                                     const long long *offs, const unsigned *psrc, unsigned *pdst)
 {
     constexpr int W = HT / 32;
     __shared__ int wcnt[W][RADIX];
@@ -136,7 +136,11 @@ __global__ void __launch_bounds__(HT) k_tile_scatter(const Tile *tiles, const un
             rtot[d] = run;
         }
         __syncthreads();
-        if (valid) dst[dbase[dg] + wcnt[wid][dg] + rank] = key;
+        if (valid) {
+            const long long pos = dbase[dg] + wcnt[wid][dg] + rank;
+            dst[pos] = key;
+            if (pdst) pdst[pos] = psrc[i];          // payload moves with its key
+        }
         __syncthreads();
         for (int d = threadIdx.x; d < RADIX; d += HT) dbase[d] += rtot[d];
         __syncthreads();
@@ -223,14 +227,20 @@ struct SortPlan {
     DevBuf<long long> seg_begin, seg_end;
     int nt = 0, nseg = 0;
     unsigned long long *out = nullptr;
+    unsigned *pout = nullptr;
 };
 
+// ordered: keys are raw double bits, sorted by value through their
+// order-preserving image (left in place); otherwise they are unsigned
+// integers.  vals/valt (nullable): a 32-bit payload moved with the keys.
 Status sort_segments(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
-                     const std::vector<long long> &len, SortPlan &sp, cudaStream_t st, int sms)
+                     const std::vector<long long> &len, SortPlan &sp, cudaStream_t st, int sms,
+                     bool ordered = true, unsigned *vals = nullptr, unsigned *valt = nullptr)
 {
     const int nseg = (int)begin.size();
     sp.nseg = nseg;
     sp.out = keys;
+    sp.pout = vals;
     std::vector<Tile> tiles;
     std::vector<int> seg_tile0((size_t)nseg + 1, 0);
     std::vector<long long> seg_end((size_t)nseg);
@@ -269,9 +279,11 @@ Status sort_segments(unsigned long long *keys, unsigned long long *alt, const st
                                    cudaMemcpyHostToDevice, st));
 
     // order-preserving image of the doubles over the used span
-    count_launch(), k_to_ordered<<<(unsigned)((hi - lo + 255) / 256 < 64 * sms ? (hi - lo + 255) / 256 : 64 * sms), 256, 0, st>>>(
-        hi - lo, keys + lo);
+    if (ordered)
+        count_launch(), k_to_ordered<<<(unsigned)((hi - lo + 255) / 256 < 64 * sms ? (hi - lo + 255) / 256 : 64 * sms), 256, 0, st>>>(
+            hi - lo, keys + lo);
     unsigned long long *a = keys, *b = alt;
+    unsigned *pa = vals, *pb = valt;
     for (int pass = 0; pass < 8; ++pass) {
         int shift = 8 * pass;
         count_launch(), k_tile_hist<<<nt, HT, 0, st>>>(sp.tiles.get(), a, shift, d_counts.get());
@@ -282,13 +294,17 @@ Status sort_segments(unsigned long long *keys, unsigned long long *alt, const st
         DRESS_CUDA_TRY(counted_memcpy(&moves, d_moves.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         if (!moves) continue;
-        count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(sp.tiles.get(), a, b, shift, d_offs.get());
+        count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(sp.tiles.get(), a, b, shift, d_offs.get(), pa, pb);
         unsigned long long *t = a;
         a = b;
         b = t;
+        unsigned *tp = pa;
+        pa = pb;
+        pb = tp;
     }
     DRESS_CUDA_TRY(cudaGetLastError());
     sp.out = a;
+    sp.pout = pa;
     return Status::Ok();
 }
 
@@ -300,6 +316,17 @@ Status segmented_sort(unsigned long long *keys, unsigned long long *alt, const s
     SortPlan sp;
     DRESS_TRY(sort_segments(keys, alt, begin, len, sp, st, sms));
     *sorted = sp.out;
+    return Status::Ok();
+}
+
+Status sort_pairs(unsigned long long *keys, unsigned long long *alt, unsigned *vals, unsigned *valt, long long n,
+                  unsigned long long **sorted_keys, unsigned **sorted_vals, cudaStream_t st, int sms)
+{
+    SortPlan sp;
+    DRESS_TRY(sort_segments(keys, alt, std::vector<long long>{0}, std::vector<long long>{n}, sp, st, sms, false,
+                            vals, valt));
+    *sorted_keys = sp.out;
+    *sorted_vals = sp.pout;
     return Status::Ok();
 }
 
@@ -652,7 +679,7 @@ extern "C" int dressx_histogram_noalloc(const double *values, int64_t n, int64_t
         const int shift = 8 * pass;
         count_launch(), k_tile_hist<<<nt, HT, 0, st>>>(tiles, a, shift, counts);
         count_launch(), k_seg_offsets<<<1, RADIX, 0, st>>>(seg_begin, seg_tile0, counts, offs, moves);
-        count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(tiles, a, b, shift, offs);
+        count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(tiles, a, b, shift, offs, nullptr, nullptr);
         unsigned long long *t = a;
         a = b;
         b = t;

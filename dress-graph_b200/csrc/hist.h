@@ -25,6 +25,12 @@ Status histogram_download(HistResult &res, std::vector<std::vector<long long>> &
 Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
                        cudaStream_t st, int sms);
 
+// Stable ascending sort of n unsigned 64-bit keys with a 32-bit payload
+// (LSD radix, 8-bit digits; digits equal on every key are skipped).  The
+// results are in whichever buffer of each pair the last pass wrote.
+Status sort_pairs(unsigned long long *keys, unsigned long long *alt, unsigned *vals, unsigned *valt, long long n,
+                  unsigned long long **sorted_keys, unsigned **sorted_vals, cudaStream_t st, int sms);
+
 // Sorts each segment [begin[s], begin[s]+len[s]) of `keys` (raw double bits,
 // replaced by their order-preserving image, see ordered_to_double) ascending;
 // *sorted is whichever of keys / alt holds the result.

@@ -82,7 +82,7 @@ class Graph:
     """Owns one ``dress_graph_t`` built by the library's ``dress_init_graph``."""
 
     def __init__(self, n_vertices, sources, targets, weights=None, vertex_weights=None,
-                 variant=UNDIRECTED, precompute_intercepts=False):
+                 variant=UNDIRECTED, precompute_intercepts=False, device_build=False):
         U = np.asarray(sources, dtype=np.int32)
         V = np.asarray(targets, dtype=np.int32)
         if U.shape != V.shape:
@@ -90,9 +90,13 @@ class Graph:
         pW = _malloc_copy(np.asarray(weights, dtype=np.float64), ctypes.c_double) if weights is not None else None
         pNW = (_malloc_copy(np.asarray(vertex_weights, dtype=np.float64), ctypes.c_double)
                if vertex_weights is not None else None)
-        self.ptr = lib().dress_init_graph(int(n_vertices), int(U.size), _malloc_copy(U, ctypes.c_int),
-                                          _malloc_copy(V, ctypes.c_int), pW, pNW, int(variant),
-                                          int(bool(precompute_intercepts)))
+        init = lib().dressx_init_graph if device_build else lib().dress_init_graph
+        pU, pV = _malloc_copy(U, ctypes.c_int), _malloc_copy(V, ctypes.c_int)
+        self.ptr = init(int(n_vertices), int(U.size), pU, pV, pW, pNW, int(variant), int(bool(precompute_intercepts)))
+        if not self.ptr:                      # the arrays stay ours on failure
+            for p in (pU, pV, pW, pNW):
+                if p:
+                    _libc.free(ctypes.cast(p, ctypes.c_void_p))
         if not self.ptr:
             raise ValueError("dress_init_graph rejected the graph (vertex id out of range?)")
         self.N = int(n_vertices)

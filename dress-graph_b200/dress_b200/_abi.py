@@ -155,6 +155,8 @@ SIGNATURES = {
     "dressx_server_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ServerStats), ctypes.c_int]),
     "dressx_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "dressx_server_estimate": (ctypes.c_int, [PGraph, ctypes.c_int, ctypes.c_int, _c_i64_p, _c_int_p]),
+    "dressx_init_graph": (PGraph, [ctypes.c_int, ctypes.c_int, _c_int_p, _c_int_p, _c_dbl_p,
+                                   _c_dbl_p, ctypes.c_int, ctypes.c_int]),
     "dressx_get_batch": (ctypes.c_int, [PGraph, _c_int_p, _c_int_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double,
                                         _c_dbl_p, ctypes.c_double, _c_dbl_p]),
     "dressx_hist_merge": (ctypes.c_int, [ctypes.POINTER(_c_i64_p), _c_i64_p, ctypes.c_int,

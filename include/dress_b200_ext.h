@@ -163,6 +163,15 @@ int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, i
 int dressx_histogram_noalloc(const double *values, int64_t n, int64_t *pairs, int64_t *num_runs,
                              void *stream);
 
+/* dress_init_graph built on the GPU: same arguments, ownership rules and
+ * result -- array for array bit-identical to the host build (and to the
+ * reference, libdress/src/dress.c:378-427) -- with the row sorting, the
+ * variant weights and the intercept tables computed on the device.  NULL on
+ * an invalid graph or a device error (dressx_last_error); the caller then
+ * keeps U, V, W and NW.  Free the result with dress_free_graph. */
+p_dress_graph_t dressx_init_graph(int N, int E, int *U, int *V, double *W, double *NW,
+                                  dress_variant_t variant, int precompute_intercepts);
+
 /* Batched virtual-edge queries on a fitted graph: out[i] is what the
  * reference's dress_get(g, u[i], v[i], max_iterations, epsilon, w) returns
  * (libdress/include/dress/dress.h:105, libdress/src/dress.c:651-739) -- the

@@ -211,3 +211,50 @@ def test_virtual_edge_query_rejects_bad_vertices():
         with pytest.raises(db.DressError) as e:
             db.get(g, [0, 60], [1, 2])
         assert e.value.code == 1
+
+
+def _graph_arrays(g):
+    c = g.ptr.contents
+    S = c.adj_offset[c.N] if c.N > 0 else 0
+    out = dict(adj_offset=db._arr(c.adj_offset, c.N + 1, np.int32), adj_target=db._arr(c.adj_target, S, np.int32),
+               adj_edge_idx=db._arr(c.adj_edge_idx, S, np.int32), edge_weight=bits(db._arr(c.edge_weight, c.E, np.float64)),
+               edge_dress=bits(db._arr(c.edge_dress, c.E, np.float64)), NW=bits(db._arr(c.NW, c.N, np.float64)),
+               max_degree=c.max_degree)
+    if c.precompute_intercepts:
+        T = c.intercept_offset[c.E]
+        out.update(intercept_offset=db._arr(c.intercept_offset, c.E + 1, np.int32),
+                   intercept_edge_ux=db._arr(c.intercept_edge_ux, T, np.int32),
+                   intercept_edge_vx=db._arr(c.intercept_edge_vx, T, np.int32))
+    return out
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_device_graph_build_matches_host(variant):
+    """dressx_init_graph (GPU) equals dress_init_graph (host, pinned to the
+    reference's construction by test_abi) array for array: simple graphs with
+    hubs, multigraphs with self loops and reciprocal edges, with and without
+    weights, vertex weights and intercept tables."""
+    rng = np.random.default_rng(variant)
+    cases = [graphs.chung_lu(3000, 20000, 2.3, 400, seed=5), graphs.erdos_renyi(500, 3000, seed=2)]
+    m = 4000
+    cases.append((300, rng.integers(0, 300, m).astype(np.int32), rng.integers(0, 300, m).astype(np.int32)))
+    cases.append((10, np.zeros(0, np.int32), np.zeros(0, np.int32)))
+    for n, U, V in cases:
+        for W, NW, pre in ((None, None, 0), (graphs.uniform_weights(len(U), seed=3), rng.uniform(0.5, 2, n), 1)):
+            with db.Graph(n, U, V, W, NW, variant, pre) as a, db.Graph(n, U, V, W, NW, variant, pre, device_build=True) as b:
+                x, y = _graph_arrays(a), _graph_arrays(b)
+                assert x.keys() == y.keys()
+                for k in x:
+                    np.testing.assert_array_equal(x[k], y[k], err_msg=f"{k} n={n} variant={variant} pre={pre}")
+
+
+def test_device_graph_build_rejects_bad_ids_and_fits_alike(oracle_port):
+    with pytest.raises(ValueError):
+        db.Graph(5, [0, 7], [1, 2], device_build=True)
+    n, U, V = graphs.chung_lu(2000, 12000, 2.3, 300, seed=8)
+    with db.Graph(n, U, V, device_build=True) as g:
+        it, dl = db.fit_graph(g, 100, 1e-6)
+        ed = g.edge_dress
+    ref = oracle_port.fit(n, U, V)
+    assert it == ref["iterations"]
+    np.testing.assert_array_equal(bits(ed), bits(ref["edge_dress"]))
