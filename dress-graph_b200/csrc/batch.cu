@@ -52,28 +52,45 @@ __device__ __forceinline__ void net(double (&a)[M])
     }
 }
 
-// Sorted KBN of the n finite terms among a[0..len) (the rest are +inf);
-// the network is the smallest power of two covering len.
-template <int M>
-__device__ __forceinline__ double sorted_sum(double (&a)[M], int len, int n)
+// Sorted KBN of the self term and the live ones among cnt stored terms
+// (term(j, t) yields stored term j and whether it is alive) in a register
+// network of Mi > cnt slots; dead and unused slots hold +inf.
+template <int Mi, class Term>
+__device__ __forceinline__ double net_sum(double self, int cnt, Term term)
 {
-    if (len <= 1) return dadd(a[0], 0.0);
-    if (len <= 2) {
-        cmx(a[0], a[1]);
-    } else if (M >= 4 && len <= 4) {
-        net<(M >= 4 ? 4 : M), M>(a);
-    } else if (M >= 8 && len <= 8) {
-        net<(M >= 8 ? 8 : M), M>(a);
-    } else if (M >= 16 && len <= 16) {
-        net<(M >= 16 ? 16 : M), M>(a);
-    } else {
-        net<M, M>(a);
+    double a[Mi];
+    a[0] = self;
+    int n = 1;
+#pragma unroll
+    for (int j = 1; j < Mi; ++j) {
+        a[j] = DRESS_INF;
+        if (j <= cnt) {
+            double t;
+            if (term(j - 1, t)) {
+                a[j] = t;
+                ++n;
+            }
+        }
     }
+    net<Mi, Mi>(a);
     double s = a[0], c = 0.0;
 #pragma unroll
-    for (int i = 1; i < M; ++i)
+    for (int i = 1; i < Mi; ++i)
         if (i < n) kbn_step(s, c, a[i]);
     return dadd(s, c);
+}
+
+// The smallest network that holds the item: most items of sparse subgraphs
+// have a handful of terms, and the cost of a network grows with its size.
+template <int M, class Term>
+__device__ __forceinline__ double item_sum(double self, int cnt, Term term)
+{
+    if (cnt == 0) return dadd(self, 0.0);
+    if (cnt < 2) return net_sum<2>(self, cnt, term);
+    if (M >= 4 && cnt < 4) return net_sum<(M >= 4 ? 4 : 2)>(self, cnt, term);
+    if (M >= 8 && cnt < 8) return net_sum<(M >= 8 ? 8 : 2)>(self, cnt, term);
+    if (M >= 16 && cnt < 16) return net_sum<(M >= 16 ? 16 : 2)>(self, cnt, term);
+    return net_sum<M>(self, cnt, term);
 }
 
 __device__ __forceinline__ long long binom_d(int n, int k)
@@ -223,19 +240,12 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
         for (int u = g.t; u < N; u += g.size) {
             if (!mk.alive(u)) continue;
             const int rb = G.row_off[u], deg = G.row_off[u + 1] - rb;
-            double a[M];
-            a[0] = dmul(4.0, mk.weight(u, G.nw));
-            int n = 1;
-#pragma unroll
-            for (int j = 1; j < M; ++j) {
-                a[j] = DRESS_INF;
-                if (j <= deg) {
-                    int e = G.row_eid[rb + j - 1];
-                    int x = G.U[e] + G.V[e] - u;
-                    if (mk.alive(x)) { a[j] = dmul(G.w[e], d0[e]); ++n; }
-                }
-            }
-            vd[u] = dsqrt(sorted_sum<M>(a, deg + 1, n));
+            vd[u] = dsqrt(item_sum<M>(dmul(4.0, mk.weight(u, G.nw)), deg, [&](int j, double &t) {
+                const int e = G.row_eid[rb + j];
+                if (!mk.alive(G.U[e] + G.V[e] - u)) return false;
+                t = dmul(G.w[e], d0[e]);
+                return true;
+            }));
         }
         g.sync();
         double lmax = 0.0;
@@ -244,23 +254,14 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
             if (!(mk.alive(u) && mk.alive(v))) continue;
             const double own = dmul(G.w[e], d0[e]);
             const double a4u = dmul(4.0, mk.weight(u, G.nw));
-            double a[M];
-            a[0] = P.fwd ? dadd(a4u, own) : dadd(dadd(a4u, dmul(4.0, mk.weight(v, G.nw))), dmul(2.0, own));
+            const double self = P.fwd ? dadd(a4u, own) : dadd(dadd(a4u, dmul(4.0, mk.weight(v, G.nw))), dmul(2.0, own));
             const int pb = G.ioff[e], np = G.ioff[e + 1] - pb;
-            int n = 1;
-#pragma unroll
-            for (int j = 1; j < M; ++j) {
-                a[j] = DRESS_INF;
-                if (j <= np) {
-                    int2 pr = G.pairs[pb + j - 1];
-                    int x = G.U[pr.x] + G.V[pr.x] - u;
-                    if (mk.alive(x)) {
-                        a[j] = dadd(dmul(G.w[pr.x], d0[pr.x]), dmul(G.w[pr.y], d0[pr.y]));
-                        ++n;
-                    }
-                }
-            }
-            const double num = sorted_sum<M>(a, np + 1, n);
+            const double num = item_sum<M>(self, np, [&](int j, double &t) {
+                const int2 pr = G.pairs[pb + j];
+                if (!mk.alive(G.U[pr.x] + G.V[pr.x] - u)) return false;
+                t = dadd(dmul(G.w[pr.x], d0[pr.x]), dmul(G.w[pr.y], d0[pr.y]));
+                return true;
+            });
             const double den = dmul(vd[u], vd[v]);
             const double r = den > 0.0 ? ddiv(num, den) : 0.0;
             d1[e] = r;
