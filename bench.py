@@ -212,6 +212,8 @@ def bench_delta1(args, rank, world, pg, torch, clocks):
     db.counters(reset=True)
     batch = db.Batch(objs, db.DELTA, 1, max_iterations=100, epsilon=1e-6)
     create = db.counters(reset=True)
+    tune = batch.autotune()              # schedule for this size class (later batches reuse it)
+    batch.capture()                      # fit stage replayed from a CUDA graph
     for _ in range(args.warmup):
         batch.run()
     ref_hist = batch.fetch()
@@ -296,7 +298,8 @@ def bench_delta1(args, rank, world, pg, torch, clocks):
                 hist_ms=hist_ms / args.steps, wall_ms=wall * 1e3 / args.steps, launches=launches,
                 e2e={"value": e2e_value, "unit": "subgraph-fits/s", "h2d_bytes_per_step": int(h2d_step),
                      "d2h_bytes_per_step": int(d2h_step), "matches_device_run": bool(same)},
-                per_fit=per_fit, roofline=roofline, clocks=clk, gs=gs_all)
+                per_fit=per_fit, roofline=roofline, clocks=clk, gs=gs_all,
+                tune={"threads_per_subgraph": tune[0], "ctas_per_sm": tune[1]})
 
 
 # ---------------------------------------------------------------------------
@@ -381,7 +384,7 @@ def bench_k2(args, clocks):
     for label, kind, k in (("delta2", db.DELTA, 2), ("nabla1", db.NABLA, 1)):
         b = db.Batch(objs, kind, k)
         t0 = time.perf_counter()
-        best, rates = b.autotune()
+        best, per_sm, rates = b.autotune()
         tune_s = time.perf_counter() - t0
         b.capture()
         b.run()                                  # warm-up
@@ -402,7 +405,8 @@ def bench_k2(args, clocks):
             "edge_sweeps_per_s": st["edge_updates"] / (fit_ms / steps / 1e3),
             "fit_ms": fit_ms / steps, "hist_ms": hist_ms / steps, "ms_per_step": step_ms,
             "gpu_launches_per_step": launches / steps,
-            "autotune": {"threads_per_subgraph": best, "sampled_fits_per_ms": rates, "seconds": tune_s},
+            "autotune": {"threads_per_subgraph": best, "ctas_per_sm": per_sm,
+                         "sampled_fits_per_ms": {f"{t}x{c}": v for (t, c), v in rates.items()}, "seconds": tune_s},
             "cuda_graph": True,
         }
         b.close()
@@ -719,7 +723,8 @@ def main():
                                    "k=1, epsilon 1e-6, max 100 sweeps, exact histogram per graph",
                        "fits_per_step": head["fits_per_step"], "edge_updates_per_step": head["edge_updates_per_step"],
                        "l2": "256 MiB flush between timed steps (outside the timed regions)",
-                       "parallelism": f"graphs sharded over {world} GPU(s)"},
+                       "parallelism": f"graphs sharded over {world} GPU(s)",
+                       "schedule": head["tune"]},
             "e2e": head["e2e"], "gpu_launches": head["launches"], "roofline": head["roofline"],
             "cpu_baseline": cpu, "per_fit_gpu": head["per_fit"],
             "breakdown_ms": {"fits": head["fit_ms"], "histograms": head["hist_ms"], "wall": head["wall_ms"]},

@@ -345,8 +345,8 @@ __device__ __forceinline__ View view_of(const unsigned char *b, const ParentLayo
 // own and reads the parent through L2, so no group idles behind another.
 // Group-mode CTAs hold at most 256 threads (several per SM), which leaves
 // the register budget of the larger networks unsplit.
-template <int M, bool GROUP>
-__global__ void __launch_bounds__(GROUP ? 256 : 512, 1) k_batch(BatchLaunch L)
+template <int M, bool GROUP, int MINB>
+__global__ void __launch_bounds__(GROUP ? 256 : 512, MINB) k_batch(BatchLaunch L)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_chunk, s_next;
@@ -404,29 +404,32 @@ __global__ void __launch_bounds__(GROUP ? 256 : 512, 1) k_batch(BatchLaunch L)
     }
 }
 
-template <int M, bool GROUP>
+template <int M, bool GROUP, int MINB>
 Status launch_mg(const BatchLaunch &L, int sms, cudaStream_t st)
 {
     if (GROUP && L.gsize * L.groups > 256)
         return Status::Err(DRESSX_EINVAL, "group-mode batch CTAs hold at most 256 threads");
     size_t smem = batch_smem_bytes(L);
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_batch<M, GROUP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_batch<M, GROUP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    DRESS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<M, GROUP>, L.gsize * L.groups, smem));
+    DRESS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<M, GROUP, MINB>, L.gsize * L.groups, smem));
     if (per_sm < 1) return Status::Err(DRESSX_EUNSUPPORTED, "batch kernel does not fit on an SM");
     long long grid = (long long)per_sm * sms;
     // no more CTAs than there are chunks (group mode: chunks per CTA = groups)
     long long need = GROUP ? (L.nchunks + L.groups - 1) / L.groups : L.nchunks;
     if (grid > need) grid = need;
-    count_launch(), k_batch<M, GROUP><<<(int)grid, L.gsize * L.groups, smem, st>>>(L);
+    count_launch(), k_batch<M, GROUP, MINB><<<(int)grid, L.gsize * L.groups, smem, st>>>(L);
     DRESS_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
 }
 
+// Two CTAs per SM (64 registers a thread) only where the networks allow it.
 template <int M>
 Status launch_m(const BatchLaunch &L, int sms, cudaStream_t st)
 {
-    return L.per_group ? launch_mg<M, true>(L, sms, st) : launch_mg<M, false>(L, sms, st);
+    if (L.per_group) return launch_mg<M, true, 1>(L, sms, st);
+    if (M <= 16 && L.min_ctas == 2) return launch_mg<M, false, (M <= 16 ? 2 : 1)>(L, sms, st);
+    return launch_mg<M, false, 1>(L, sms, st);
 }
 
 }  // namespace

@@ -73,6 +73,7 @@ struct BatchLaunch {
     int gsize, groups;               // threads per subgraph, subgraphs per CTA
     int stage;                       // parents copied into shared memory (CTA mode)
     int per_group;                   // every group takes its own chunks (no staging)
+    int min_ctas;                    // CTAs per SM the schedule is built for (1 or 2)
     int maxE, maxN, maxk;            // per-group state sizes
     long long parent_bytes;          // staging area size
     int M;                           // register network size (max terms)

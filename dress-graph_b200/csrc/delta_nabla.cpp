@@ -328,6 +328,7 @@ Status hist_of_host_values(std::vector<Prep *> &ps, cudaStream_t st, int sms)
 // ---- batched path ------------------------------------------------------------------
 struct Tune {
     int gsize, groups;
+    int per_sm = 1;          // CTAs meant to share an SM (shared memory split between them)
 };
 
 // Threads per subgraph by edge count (sweeps of a few hundred edges keep a
@@ -341,7 +342,7 @@ struct TuneKey {
     }
 };
 std::mutex g_tuned_mu;
-std::map<TuneKey, int> g_tuned;     // size class -> measured best threads per subgraph
+std::map<TuneKey, Tune> g_tuned;    // size class -> measured best schedule
 
 TuneKey tune_key(int maxE, int maxN, int M, int maxk)
 {
@@ -355,18 +356,22 @@ Tune pick_tune(int maxE, int maxN, int M, int maxk, const dressx_config_t &cfg)
     if (cfg.group_threads <= 0) {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
         auto it = g_tuned.find(tune_key(maxE, maxN, M, maxk));
-        if (it != g_tuned.end()) gs = it->second;
+        if (it != g_tuned.end()) return it->second;
     }
     int groups = 512 / gs;
     if (gs > 32 && groups > 15) groups = 15;
-    return {gs, groups};
+    return {gs, groups, 1};
 }
 
 // Groups per CTA and parent staging for a given group size: as many groups
 // as shared memory holds (at most `groups`), staging the parent unless that
 // halves the groups.  False when not even one group fits.
-bool shape_launch(BatchLaunch &L, const Tune &tu, long long smem_cap)
+bool shape_launch(BatchLaunch &L, const Tune &tu, long long smem_cap_full, long long smem_sm = 0)
 {
+    // two CTAs per SM split the SM's shared memory (each keeps ~1 KB of
+    // system and static shared memory)
+    const long long smem_cap = tu.per_sm == 2 && smem_sm > 0 ? smem_sm / 2 - 2048 : smem_cap_full;
+    L.min_ctas = tu.per_sm == 2 && smem_sm > 0 && L.M <= 16 ? 2 : 1;
     L.gsize = tu.gsize;
     L.per_group = 0;
     L.stage = 1;
@@ -424,7 +429,8 @@ struct BatchPlan {
     HistResult hist;
     bool need_hist = false;
     float fit_ms = 0.f, hist_ms = 0.f;       // device time of the last run
-    long long smem_cap = 0;
+    long long smem_cap = 0, smem_sm = 0;
+    int tuned_per_sm = 1;                    // CTAs per SM the autotuner chose
     cudaGraphExec_t gexec = nullptr;         // captured fit stage (dressx_batch_capture)
     ~BatchPlan()
     {
@@ -482,7 +488,10 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
     L.M = M;
     L.parent_bytes = maxbytes;
     P.smem_cap = smem_cap;
-    if (!shape_launch(L, tu, smem_cap))
+    int smem_sm = 0;
+    DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, en.device));
+    P.smem_sm = smem_sm;
+    if (!shape_launch(L, tu, smem_cap, smem_sm))
         return Status::Err(DRESSX_EUNSUPPORTED, "subgraph state exceeds shared memory");
 
     // pack parents
@@ -654,8 +663,13 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
     long long total = 0;
     for (Prep *p : P.ps) total += p->items;
     if (total == 0) return Status::Ok();
-    const long long limit = total <= 3 * 16384 ? total : std::max<long long>(16384, total / 10);
-    const int cands[4] = {32, 64, 128, 256};
+    // the whole batch up to 200K subgraphs (a sample leaves too few chunks per
+    // SM to show the tail of a schedule), a spread quarter beyond
+    const long long limit = total <= 200000 ? total : std::max<long long>(200000, total / 4);
+    struct Cand { int gs, per_sm; };
+    std::vector<Cand> cands = {{32, 1}, {64, 1}, {128, 1}, {256, 1}};
+    if (P.L.M <= 16)                      // the kernel fits two 512-thread CTAs per SM there
+        for (int gs : {32, 64, 128}) cands.push_back({gs, 2});
     DevBuf<Chunk> d_try;
     cudaEvent_t e0, e1;
     DRESS_CUDA_TRY(cudaEventCreate(&e0));
@@ -663,15 +677,20 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
     int best = -1;
     double best_rate = 0.0;
     Status err;
-    for (int gs : cands) {
-        Tune tu{gs, gs == 32 ? 16 : std::min(15, 512 / gs)};
+    Tune best_tu{0, 0, 1};
+    for (const Cand &cd : cands) {
+        const int gs = cd.gs;
+        Tune tu{gs, gs == 32 ? 16 : std::min(15, 512 / gs), cd.per_sm};
         BatchLaunch L = P.L;
-        if (!shape_launch(L, tu, P.smem_cap)) {
+        if (!shape_launch(L, tu, P.smem_cap, P.smem_sm)) {
             if (rates) rates->push_back(0.f);
             continue;
         }
-        std::vector<Chunk> ch;
-        build_chunks(P.ps, L.groups, limit, ch);
+        // a sample spread over the whole batch: every k-th chunk
+        std::vector<Chunk> all, ch;
+        build_chunks(P.ps, L.groups, -1, all);
+        const long long k = std::max<long long>(1, (total + limit - 1) / limit);
+        for (size_t c = 0; c < all.size(); c += (size_t)k) ch.push_back(all[c]);
         long long items = 0;
         for (const Chunk &c : ch) items += c.count;
         err = d_try.alloc(ch.size(), st);
@@ -683,7 +702,8 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
         L.chunks = d_try.get();
         L.nchunks = (int)ch.size();
         float ms = 0.f;
-        for (int rep = 0; rep < 2; ++rep) {          // the first run is untimed
+        float best_ms = 0.f;
+        for (int rep = 0; rep < 3; ++rep) {          // the first run is untimed; the faster of two
             cudaMemsetAsync(P.d_stats.get(), 0, ST_WORDS * P.ps.size() * sizeof(unsigned long long), st);
             cudaMemsetAsync(P.d_counter.get(), 0, sizeof(int), st);
             cudaEventRecord(e0, st);
@@ -695,13 +715,15 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
                 break;
             }
             cudaEventElapsedTime(&ms, e0, e1);
+            if (rep == 1 || (rep > 1 && ms < best_ms)) best_ms = ms;
         }
         if (!err.ok()) break;
-        const double rate = ms > 0.f ? (double)items / ms : 0.0;
+        const double rate = best_ms > 0.f ? (double)items / best_ms : 0.0;
         if (rates) rates->push_back((float)rate);
         if (rate > best_rate) {
             best_rate = rate;
             best = gs;
+            best_tu = tu;
         }
     }
     cudaEventDestroy(e0);
@@ -710,10 +732,11 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
     if (best < 0) return Status::Err(DRESSX_EUNSUPPORTED, "autotune: no group size fits");
     {
         std::lock_guard<std::mutex> lk(g_tuned_mu);
-        g_tuned[tune_key(P.L.maxE, P.L.maxN, P.L.M, P.L.maxk)] = best;
+        g_tuned[tune_key(P.L.maxE, P.L.maxN, P.L.M, P.L.maxk)] = best_tu;
     }
-    Tune tu{best, best == 32 ? 16 : std::min(15, 512 / best)};
-    if (!shape_launch(P.L, tu, P.smem_cap)) return Status::Err(DRESSX_EUNSUPPORTED, "autotune: re-plan failed");
+    if (!shape_launch(P.L, best_tu, P.smem_cap, P.smem_sm))
+        return Status::Err(DRESSX_EUNSUPPORTED, "autotune: re-plan failed");
+    P.tuned_per_sm = best_tu.per_sm;
     build_chunks(P.ps, P.L.groups, -1, P.chunks);
     DRESS_TRY(P.d_chunks.alloc(P.chunks.size(), st));
     DRESS_CUDA_TRY(counted_memcpy(P.d_chunks.get(), P.chunks.data(), P.chunks.size() * sizeof(Chunk),
@@ -1086,7 +1109,7 @@ int dressx_batch_run(dressx_batch_t *b)
     return s.code;
 }
 
-int dressx_batch_autotune(dressx_batch_t *b, int *group_threads, float *rates)
+int dressx_batch_autotune(dressx_batch_t *b, int *group_threads, int *ctas_per_sm, float *rates)
 {
     if (!b) return DRESSX_EINVAL;
     Engine &en = engine();
@@ -1095,8 +1118,9 @@ int dressx_batch_autotune(dressx_batch_t *b, int *group_threads, float *rates)
     int best = b->ptrs.empty() ? 0 : b->plan.L.gsize;
     Status s = b->ptrs.empty() ? Status::Ok() : autotune_batched(b->plan, en.ctx, &best, &r);
     if (group_threads) *group_threads = best;
+    if (ctas_per_sm) *ctas_per_sm = b->plan.tuned_per_sm;
     if (rates)
-        for (int i = 0; i < 4; ++i) rates[i] = i < (int)r.size() ? r[(size_t)i] : 0.f;
+        for (int i = 0; i < 8; ++i) rates[i] = i < (int)r.size() ? r[(size_t)i] : 0.f;
     set_last_error(s);
     return s.code;
 }

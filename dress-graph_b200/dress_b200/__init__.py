@@ -349,12 +349,14 @@ class Batch:
         _check(lib().dressx_batch_run(self.handle))
 
     def autotune(self):
-        """Measure 32/64/128/256 threads per subgraph on a sample, keep the
-        fastest.  Returns (threads, {threads: sampled fits per ms})."""
-        gt = ctypes.c_int()
-        rates = (ctypes.c_float * 4)()
-        _check(lib().dressx_batch_autotune(self.handle, ctypes.byref(gt), rates))
-        return gt.value, {t: float(r) for t, r in zip((32, 64, 128, 256), rates)}
+        """Measure the batch kernel's schedules on a sample, keep the fastest.
+        Returns (threads per subgraph, CTAs per SM, {(threads, CTAs per SM):
+        sampled fits per ms})."""
+        gt, cps = ctypes.c_int(), ctypes.c_int()
+        rates = (ctypes.c_float * 8)()
+        _check(lib().dressx_batch_autotune(self.handle, ctypes.byref(gt), ctypes.byref(cps), rates))
+        keys = [(32, 1), (64, 1), (128, 1), (256, 1), (32, 2), (64, 2), (128, 2)]
+        return gt.value, cps.value, {k: float(r) for k, r in zip(keys, rates)}
 
     def capture(self):
         """Capture the fit stage into a CUDA graph replayed by ``run()``."""

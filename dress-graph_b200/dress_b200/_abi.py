@@ -140,7 +140,7 @@ SIGNATURES = {
     "dressx_batch_create": (ctypes.c_int, [ctypes.POINTER(HistRequest), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "dressx_batch_run": (ctypes.c_int, [ctypes.c_void_p]),
     "dressx_batch_fetch": (ctypes.c_int, [ctypes.c_void_p]),
-    "dressx_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, ctypes.POINTER(ctypes.c_float)]),
+    "dressx_batch_autotune": (ctypes.c_int, [ctypes.c_void_p, _c_int_p, _c_int_p, ctypes.POINTER(ctypes.c_float)]),
     "dressx_batch_capture": (ctypes.c_int, [ctypes.c_void_p]),
     "dressx_batch_stats": (ctypes.c_int, [ctypes.c_void_p, _c_i64_p, _c_i64_p, _c_i64_p]),
     "dressx_batch_timing": (ctypes.c_int, [ctypes.c_void_p, _c_dbl_p, _c_dbl_p]),

@@ -176,8 +176,9 @@ def test_autotuned_and_captured_batch_matches(kind, k):
     objs = [db.Graph(n, U, V) for n, U, V in gs]
     expect = [r[0] for r in db.hist_requests(objs, kind, k)]
     b = db.Batch(objs, kind, k)
-    best, rates = b.autotune()
-    assert best in (32, 64, 128, 256) and rates[best] == max(rates.values()) > 0
+    best, per_sm, rates = b.autotune()
+    assert best in (32, 64, 128, 256) and per_sm in (1, 2)
+    assert rates[(best, per_sm)] == max(rates.values()) > 0
     b.run()
     for x, y in zip(b.fetch(), expect):
         np.testing.assert_array_equal(x, y)
