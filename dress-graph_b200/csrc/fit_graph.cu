@@ -36,7 +36,6 @@
 namespace dress {
 namespace {
 
-constexpr int RING = 64;           // per-sweep convergence slots
 constexpr int MAX_CHUNK = 32;      // sweeps launched per host check (<= RING/2)
 using namespace sweep;
 
@@ -672,25 +671,65 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + E};
     double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + E};
 
-    // per-sweep max|delta| slots form a ring; a chunk zeroes its own slots
-    // first, and the first sweep of a chunk still sees the previous slot
+    // Two sweeps (the even one writes buffer 1, the odd one buffer 0) and the
+    // index steps between them are captured once into a CUDA graph, replayed
+    // for every pair of sweeps; the host reads the ring after each chunk.
+    DevBuf<int> d_iter;
+    DRESS_TRY(d_iter.alloc(1, st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_iter.get(), 0, sizeof(int), st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_maxd.get(), 0, RING * sizeof(unsigned long long), st));
+    s.iter = d_iter.get();
+    s.max_iter = max_iterations;
+    Sweep sw2[2] = {s, s};
+    for (int par = 0; par < 2; ++par) {
+        sw2[par].d = dbuf[par]; sw2[par].dn = dbuf[par ^ 1];
+        sw2[par].p = pbuf[par]; sw2[par].pn = pbuf[par ^ 1];
+    }
+    auto enqueue_pair = [&]() -> Status {
+        for (int par = 0; par < 2; ++par) {
+            if (uniform) DRESS_TRY(launch_sweep<true>(sw2[par], vb, eb, lc));
+            else         DRESS_TRY(launch_sweep<false>(sw2[par], vb, eb, lc));
+            count_launch(), k_next_sweep<<<1, 1, 0, st>>>(d_iter.get(), d_maxd.get());
+            DRESS_CUDA_TRY(cudaGetLastError());
+        }
+        return Status::Ok();
+    };
+    cudaGraphExec_t gexec = nullptr;
+    long long pair_launches = 0;
+    {
+        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+        const long long before = engine().launches.load();
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            Status cs = enqueue_pair();
+            cudaError_t e = cudaStreamEndCapture(st, &graph);
+            if (cs.ok() && e == cudaSuccess && graph && cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess)
+                gexec = nullptr;
+            if (graph) cudaGraphDestroy(graph);
+        }
+        cudaGetLastError();                           // a failed capture leaves direct launches
+        pair_launches = engine().launches.load() - before;
+        engine().launches -= pair_launches;           // counted per replay below
+    }
+    struct GraphGuard {
+        cudaGraphExec_t g;
+        ~GraphGuard() { if (g) cudaGraphExecDestroy(g); }
+    } guard{gexec};
     unsigned long long hmax[RING];
     int conv = -1, done = 0;
     int chunk = ctx.cfg->fit_chunk > 0 ? (ctx.cfg->fit_chunk < MAX_CHUNK ? ctx.cfg->fit_chunk : MAX_CHUNK) : 8;
+    chunk = (chunk + 1) & ~1;
     double last_delta = 0.0;
     while (done < max_iterations && conv < 0) {
-        int hi = done + chunk < max_iterations ? done + chunk : max_iterations;
-        for (int it = done; it < hi; ++it)
-            DRESS_CUDA_TRY(cudaMemsetAsync(d_maxd.get() + it % RING, 0, sizeof(unsigned long long), st));
-        for (int it = done; it < hi; ++it) {
-            s.iter = it;
-            s.slot = it % RING;
-            s.prev_slot = (it + RING - 1) % RING;
-            s.d = dbuf[it & 1]; s.dn = dbuf[(it + 1) & 1];
-            s.p = pbuf[it & 1]; s.pn = pbuf[(it + 1) & 1];
-            if (uniform) DRESS_TRY(launch_sweep<true>(s, vb, eb, lc));
-            else         DRESS_TRY(launch_sweep<false>(s, vb, eb, lc));
+        for (int r = 0; r < chunk / 2; ++r) {
+            if (gexec) {
+                count_launch((int)pair_launches);
+                DRESS_CUDA_TRY(cudaGraphLaunch(gexec, st));
+            } else {
+                DRESS_TRY(enqueue_pair());
+            }
         }
+        const int hi = done + chunk < max_iterations ? done + chunk : max_iterations;
         DRESS_CUDA_TRY(counted_memcpy(hmax, d_maxd.get(), RING * sizeof(unsigned long long),
                                        cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -701,7 +740,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
             if (m < epsilon) { conv = it; break; }
         }
         done = hi;
-        if (chunk < 32) chunk *= 2;
+        if (chunk < MAX_CHUNK) chunk *= 2;
     }
     const int last = conv >= 0 ? conv : max_iterations - 1;
     // device time of the sweeps (the chunk tails after convergence return at once)

@@ -76,7 +76,8 @@ struct Sweep {
     unsigned long long *maxd;      // convergence ring
     const double *d, *p;           // current values and products
     double *dn, *pn;               // next values and products
-    int iter, slot, prev_slot;     // sweep index and its convergence slots
+    const int *iter;               // device: index of the sweep being run
+    int max_iter;                  // sweeps at or past it return at once
     double eps;
     double *scratch_k;             // block-bin spill (keys), per block
     int2 *scratch_v;               // block-bin spill (payload), per block
@@ -90,9 +91,26 @@ struct Sweep {
     long long sbase, tbase;        // row slot / pair offset minus these bases
 };
 
+// Per-sweep max|delta| slots form a ring; the sweep index lives in device
+// memory, so every sweep of a chunk is the same launch sequence (replayed from
+// a CUDA graph) and the sweeps after convergence return at once.
+constexpr int RING = 64;
+
 __device__ __forceinline__ bool skipped(const Sweep &s)
 {
-    return s.iter > 0 && __longlong_as_double((long long)s.maxd[s.prev_slot]) < s.eps;
+    const int it = *s.iter;
+    return it >= s.max_iter ||
+           (it > 0 && __longlong_as_double((long long)s.maxd[(it + RING - 1) % RING]) < s.eps);
+}
+
+__device__ __forceinline__ unsigned long long *max_slot(const Sweep &s) { return &s.maxd[*s.iter % RING]; }
+
+// end of a sweep: the next index, its slot cleared
+__global__ void k_next_sweep(int *iter, unsigned long long *maxd)
+{
+    const int it = *iter + 1;
+    *iter = it;
+    maxd[it % RING] = 0ULL;
 }
 
 template <bool UNIF>
@@ -490,7 +508,7 @@ __global__ void __launch_bounds__(128) k_edge_thr(Sweep s, int begin, int end)
         }
         delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, num));
     }
-    block_max_to(&s.maxd[s.slot], delta);
+    block_max_to(max_slot(s), delta);
 }
 
 // ---- one thread per item, streamed (at most MED_CAP stored terms) ---------------------
@@ -534,7 +552,7 @@ __global__ void __launch_bounds__(256) k_edge_med(Sweep s, int begin, int end)
         else
             s.qe[atomicAdd(&s.qcount[1], 1u)] = j;
     }
-    block_max_to(&s.maxd[s.slot], delta);
+    block_max_to(max_slot(s), delta);
 }
 
 // one warp per queued item: restore ascending order, write it back, and sum
@@ -631,7 +649,7 @@ __global__ void __launch_bounds__(128) k_edge_med_sum(Sweep s)
         delta = fmax(delta, finish_edge<UNIF>(s, j, u, v, kbn_merge_stream(s.tkey + (o - s.tbase), nc,
                                                                           self_term<UNIF>(s, j, u, v))));
     }
-    block_max_to(&s.maxd[s.slot], delta);
+    block_max_to(max_slot(s), delta);
 }
 
 // ---- one block per item (hub rows, hub edges) -----------------------------------------
@@ -719,7 +737,7 @@ __global__ void __launch_bounds__(512) k_edge_block(Sweep s, int begin, int end,
         }
         __syncthreads();
     }
-    if (SUM_HERE) block_max_to(&s.maxd[s.slot], delta);
+    if (SUM_HERE) block_max_to(max_slot(s), delta);
 }
 
 // The sequential sums of the block items' sorted slots, in 32-thread
@@ -762,7 +780,7 @@ __global__ void __launch_bounds__(32) k_edge_block_sum(Sweep s, int big0, int nb
         delta = finish_edge<UNIF>(s, j, u, v, kbn_merge_stream(s.bkey_e + s.bofs_e[j - s.be0], nc,
                                                                self_term<UNIF>(s, j, u, v)));
     }
-    block_max_to(&s.maxd[s.slot], delta);
+    block_max_to(max_slot(s), delta);
 }
 
 // ---- launch of one sweep ------------------------------------------------------------
