@@ -101,6 +101,12 @@ __global__ void k_directed(long long R, const unsigned long long *key, const uns
     }
 }
 
+__global__ void k_iota(long long n, unsigned *out)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (unsigned)i;
+}
+
 // the CSR from the sorted slots; wmode 0: w-bar = 2w, 1: w, 2: per-slot weights
 __global__ void k_csr(long long S, int und_ids, const unsigned long long *key, const unsigned *id,
                       const unsigned *vedge, const double *vw, const double *W, int wmode, int *tgt, int *eidx,
@@ -252,9 +258,7 @@ Status build(p_dress_graph_t g, const Ctx &ctx)
         count_launch(), k_directed<<<grid1(R, sms), 256, 0, st>>>(R, rk, ri, d_roff.get(), g->W ? d_W.get() : nullptr,
                                                                    vk0.get(), d_vedge.get(), d_vw.get());
         // payload = emission index, in emission order
-        std::vector<unsigned> iota((size_t)(2 * R));
-        for (long long q = 0; q < 2 * R; ++q) iota[(size_t)q] = (unsigned)q;
-        DRESS_CUDA_TRY(counted_memcpy(vi0.get(), iota.data(), (size_t)(2 * R) * 4, cudaMemcpyHostToDevice, st));
+        count_launch(), k_iota<<<grid1(2 * R, sms), 256, 0, st>>>(2 * R, vi0.get());
         unsigned long long *sk;
         unsigned *si;
         DRESS_TRY(sort_pairs(vk0.get(), vk1.get(), vi0.get(), vi1.get(), 2 * R, &sk, &si, st, sms));
