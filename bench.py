@@ -364,6 +364,31 @@ def bench_single_fit(args, torch):
                          "algorithmic_bytes_per_sweep": b_iter},
         }
         g.close()
+    if not args.single_fit_only:
+        # the reference's CPU fits on the same weighted graph, a bounded number
+        # of sweeps (epsilon 0 runs exactly that many)
+        import ctypes
+        import oracle
+        cpu = oracle.reference()
+        kind = "reference" if cpu is not None else "port"
+        cpu = cpu or oracle.port()
+        t0 = time.perf_counter()
+        gr = cpu.build(n, U, V, graphs.uniform_weights(E, seed=7))
+        build_s = time.perf_counter() - t0
+        it_, dl_ = ctypes.c_int(), ctypes.c_double()
+        res = {}
+        for label, fn, sweeps in (("omp", getattr(cpu, "fit_omp", None), 2), ("single_thread", cpu.fit_fn, 1)):
+            if fn is None:
+                continue
+            t0 = time.perf_counter()
+            fn(gr, sweeps, 0.0, ctypes.byref(it_), ctypes.byref(dl_))
+            dt = time.perf_counter() - t0
+            res[label] = {"value": E * sweeps / dt, "unit": "edge-iters/s", "ms_per_sweep": dt * 1e3 / sweeps,
+                          "cores": len(os.sched_getaffinity(0)) if label == "omp" else 1, "kind": kind,
+                          "sample": f"{sweeps} sweep(s) of the weighted fit (epsilon 0)"}
+        cpu.free_graph(gr)
+        res["graph_build_s"] = build_s
+        out["cpu_baseline"] = res
     return out
 
 
