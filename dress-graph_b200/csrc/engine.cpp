@@ -57,8 +57,10 @@ Status Ctx::create(int dev, int sms, const dressx_config_t *config, int priority
     cfg = config;
     DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority));
     DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, priority));
+    DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&side2, cudaStreamNonBlocking, priority));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join2, cudaEventDisableTiming));
     return Status::Ok();
 }
 
@@ -66,12 +68,15 @@ void Ctx::destroy()
 {
     if (st) cudaStreamSynchronize(st);
     if (side) cudaStreamSynchronize(side);
+    if (side2) cudaStreamSynchronize(side2);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
+    if (join2) cudaEventDestroy(join2);
     if (st) cudaStreamDestroy(st);
     if (side) cudaStreamDestroy(side);
-    st = side = nullptr;
-    fork = join = nullptr;
+    if (side2) cudaStreamDestroy(side2);
+    st = side = side2 = nullptr;
+    fork = join = join2 = nullptr;
 }
 
 Status Engine::init()

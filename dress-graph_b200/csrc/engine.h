@@ -101,7 +101,8 @@ struct Ctx {
     int num_sms = 148;
     cudaStream_t st = nullptr;             // main stream
     cudaStream_t side = nullptr;           // concurrent hub work of the single-graph fit
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t side2 = nullptr;          // ... and its block items below the hubs
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
     const dressx_config_t *cfg = nullptr;
     // priority: CUDA stream priority of both streams (0 = default; lower
     // numbers are served first by the block scheduler)

@@ -803,8 +803,8 @@ struct LaunchCfg {
     int sms;
     int block_cap;                  // BBIG edges: stored terms in shared memory (16 B each)
     int vblock_cap;                 // BBIG rows: stored terms in shared memory (12 B each)
-    cudaStream_t st, side;          // thread/streamed items on st, block items on side
-    cudaEvent_t fork, join;
+    cudaStream_t st, side, side2;   // thread/streamed items on st; hubs on side, other block items on side2
+    cudaEvent_t fork, join, join2;
 };
 
 constexpr int THR = 128;
@@ -831,30 +831,50 @@ Status set_sweep_attributes(int block_cap, int vblock_cap)
 template <bool UNIF, bool EDGE>
 void launch_blocks(const Sweep &s, const Bins &b, const LaunchCfg &c)
 {
-    if (b.has(BBIG)) {
-        if (EDGE)
-            count_launch(), k_edge_block<UNIF, false><<<grid_for(b.count(BBIG), 1, c.sms), 512, (size_t)c.block_cap * 16,
-                                                  c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.block_cap);
-        else
-            count_launch(), k_vertex_block<UNIF, false><<<grid_for(b.count(BBIG), 1, c.sms), 512, (size_t)c.vblock_cap * 12,
-                                                    c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.vblock_cap);
-    }
-    if (b.has(BBLOCK)) {
-        if (EDGE)
-            count_launch(), k_edge_block<UNIF, false><<<grid_for(b.count(BBLOCK), 1, 3 * c.sms), 512, (size_t)BIG_CAP * 16,
-                                                 c.side>>>(s, b.start[BBLOCK], b.start[BBLOCK + 1], BIG_CAP);
-        else
-            count_launch(), k_vertex_block<UNIF, false><<<grid_for(b.count(BBLOCK), 1, 4 * c.sms), 512, (size_t)BIG_CAP * 12,
-                                                   c.side>>>(s, b.start[BBLOCK], b.start[BBLOCK + 1], BIG_CAP);
-    }
+    // the hubs' sorts and sums on one stream, so their long chains start as
+    // early as possible; the smaller block items beside them on another
     const int nblk = b.count(BBLOCK), nbig = b.count(BBIG);
-    if (nblk + nbig > 0) {
-        const unsigned g = (unsigned)(nbig + (nblk + 31) / 32);
-        if (EDGE)
-            count_launch(), k_edge_block_sum<UNIF><<<g, 32, 0, c.side>>>(s, b.start[BBIG], nbig, b.start[BBLOCK], nblk);
-        else
-            count_launch(), k_vertex_block_sum<UNIF><<<g, 32, 0, c.side>>>(s, b.start[BBIG], nbig, b.start[BBLOCK], nblk);
+    if (nbig > 0) {
+        if (EDGE) {
+            count_launch(), k_edge_block<UNIF, false><<<grid_for(nbig, 1, c.sms), 512, (size_t)c.block_cap * 16,
+                                                  c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.block_cap);
+            count_launch(), k_edge_block_sum<UNIF><<<nbig, 32, 0, c.side>>>(s, b.start[BBIG], nbig, 0, 0);
+        } else {
+            count_launch(), k_vertex_block<UNIF, false><<<grid_for(nbig, 1, c.sms), 512, (size_t)c.vblock_cap * 12,
+                                                    c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.vblock_cap);
+            count_launch(), k_vertex_block_sum<UNIF><<<nbig, 32, 0, c.side>>>(s, b.start[BBIG], nbig, 0, 0);
+        }
     }
+    if (nblk > 0) {
+        const unsigned g = (unsigned)((nblk + 31) / 32);
+        if (EDGE) {
+            count_launch(), k_edge_block<UNIF, false><<<grid_for(nblk, 1, 3 * c.sms), 512, (size_t)BIG_CAP * 16,
+                                                 c.side2>>>(s, b.start[BBLOCK], b.start[BBLOCK + 1], BIG_CAP);
+            count_launch(), k_edge_block_sum<UNIF><<<g, 32, 0, c.side2>>>(s, 0, 0, b.start[BBLOCK], nblk);
+        } else {
+            count_launch(), k_vertex_block<UNIF, false><<<grid_for(nblk, 1, 4 * c.sms), 512, (size_t)BIG_CAP * 12,
+                                                   c.side2>>>(s, b.start[BBLOCK], b.start[BBLOCK + 1], BIG_CAP);
+            count_launch(), k_vertex_block_sum<UNIF><<<g, 32, 0, c.side2>>>(s, 0, 0, b.start[BBLOCK], nblk);
+        }
+    }
+}
+
+// fork the side streams off st / join them back
+inline Status fork_sides(const LaunchCfg &c)
+{
+    DRESS_CUDA_TRY(cudaEventRecord(c.fork, c.st));
+    DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
+    DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side2, c.fork, 0));
+    return Status::Ok();
+}
+
+inline Status join_sides(const LaunchCfg &c)
+{
+    DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
+    DRESS_CUDA_TRY(cudaEventRecord(c.join2, c.side2));
+    DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
+    DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join2, 0));
+    return Status::Ok();
 }
 
 // Streamed items: one pass over all of them, then the queued ones sorted and finished.
@@ -885,8 +905,7 @@ Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, const Launch
     DRESS_CUDA_TRY(cudaMemsetAsync(s.qcount, 0, 2 * sizeof(unsigned), c.st));
     const bool vside = vb.has(BBLOCK) || vb.has(BBIG);
     if (vside) {
-        DRESS_CUDA_TRY(cudaEventRecord(c.fork, c.st));
-        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
+        DRESS_TRY(fork_sides(c));
         launch_blocks<UNIF, false>(s, vb, c);
     }
     launch_med<UNIF, false>(s, vb, c);
@@ -895,14 +914,10 @@ Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, const Launch
     if (vb.has(B4)) count_launch(), k_vertex_thr<4, UNIF><<<grid_for(vb.count(B4), THR, 16 * c.sms), THR, 0, c.st>>>(s, vb.start[B4], vb.start[B4 + 1]);
     if (vb.has(B2)) count_launch(), k_vertex_thr<2, UNIF><<<grid_for(vb.count(B2), THR, 16 * c.sms), THR, 0, c.st>>>(s, vb.start[B2], vb.start[B2 + 1]);
     if (vb.has(B0)) count_launch(), k_vertex_thr<0, UNIF><<<grid_for(vb.count(B0), THR, 16 * c.sms), THR, 0, c.st>>>(s, vb.start[B0], vb.start[B0 + 1]);
-    if (vside) {
-        DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
-        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
-    }
+    if (vside) DRESS_TRY(join_sides(c));
     const bool eside = eb.has(BBLOCK) || eb.has(BBIG);
     if (eside) {
-        DRESS_CUDA_TRY(cudaEventRecord(c.fork, c.st));
-        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
+        DRESS_TRY(fork_sides(c));
         launch_blocks<UNIF, true>(s, eb, c);
     }
     launch_med<UNIF, true>(s, eb, c);
@@ -911,10 +926,7 @@ Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, const Launch
     if (eb.has(B4)) count_launch(), k_edge_thr<4, UNIF><<<grid_for(eb.count(B4), THR, 16 * c.sms), THR, 0, c.st>>>(s, eb.start[B4], eb.start[B4 + 1]);
     if (eb.has(B2)) count_launch(), k_edge_thr<2, UNIF><<<grid_for(eb.count(B2), THR, 16 * c.sms), THR, 0, c.st>>>(s, eb.start[B2], eb.start[B2 + 1]);
     if (eb.has(B0)) count_launch(), k_edge_thr<0, UNIF><<<grid_for(eb.count(B0), THR, 16 * c.sms), THR, 0, c.st>>>(s, eb.start[B0], eb.start[B0 + 1]);
-    if (eside) {
-        DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
-        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
-    }
+    if (eside) DRESS_TRY(join_sides(c));
     DRESS_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
 }
