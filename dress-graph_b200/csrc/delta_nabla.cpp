@@ -19,14 +19,17 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "batch.h"
 #include "engine.h"
 #include "hist.h"
+#include "host_par.h"
 
 namespace dress {
 
@@ -494,15 +497,25 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
     if (!shape_launch(L, tu, smem_cap, smem_sm))
         return Status::Err(DRESSX_EUNSUPPORTED, "subgraph state exceeds shared memory");
 
-    // pack parents
-    std::vector<unsigned char> hbytes((size_t)arena);
-    std::vector<long long> hranks;
-    hranks.reserve((size_t)nranks);
-    for (size_t i = 0; i < ps.size(); ++i) {
+    // pack parents, several threads for many, into the pinned stage when it
+    // can hold them (the upload is then one DMA; the stage is free again
+    // when this function returns)
+    unsigned char *hbytes = nullptr;
+    std::unique_ptr<unsigned char[]> hheap;
+    const bool staged = en.stage && en.stage->reserve((size_t)arena).ok();
+    if (staged) {
+        hbytes = (unsigned char *)en.stage->ptr();
+    } else {
+        hheap.reset(new unsigned char[(size_t)arena]);
+        hbytes = hheap.get();
+    }
+    std::vector<long long> hranks((size_t)nranks);
+    parallel_for((long long)ps.size(), host_threads((long long)ps.size() / 16), [&](long long ii) {
+        const size_t i = (size_t)ii;
         Prep *p = ps[i];
         p_dress_graph_t g = p->g;
         ParentLayout PL = parent_layout(p->N, p->E, p->S, p->T, 0, 0);
-        unsigned char *b = hbytes.data() + data_off[i];
+        unsigned char *b = hbytes + data_off[i];
         std::memcpy(b + PL.U, g->U, (size_t)p->E * 4);
         std::memcpy(b + PL.V, g->V, (size_t)p->E * 4);
         std::memcpy(b + PL.w, g->edge_weight, (size_t)p->E * 8);
@@ -510,8 +523,8 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
         std::memcpy(b + PL.row_eid, g->adj_edge_idx, (size_t)p->S * 4);
         std::memcpy(b + PL.ioff, p->ioff.data(), (size_t)(p->E + 1) * 4);
         if (p->T) std::memcpy(b + PL.pairs, p->pairs.data(), (size_t)p->T * 8);
-        hranks.insert(hranks.end(), p->ranks.begin(), p->ranks.end());
-    }
+        if (!p->ranks.empty()) std::copy(p->ranks.begin(), p->ranks.end(), hranks.begin() + ranks_off[i]);
+    }, 16);
     std::vector<Chunk> &chunks = P.chunks;
     build_chunks(ps, L.groups, -1, chunks);
 
@@ -541,7 +554,7 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
         d.multisets = ms_off[(size_t)i] >= 0 ? d_ms.get() + ms_off[(size_t)i] : nullptr;
         d.ranks = ranks_off[(size_t)i] >= 0 ? d_ranks.get() + ranks_off[(size_t)i] : nullptr;
     }
-    DRESS_CUDA_TRY(counted_memcpy(d_pdata.get(), hbytes.data(), (size_t)arena, cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(counted_memcpy(d_pdata.get(), hbytes, (size_t)arena, cudaMemcpyHostToDevice, st));
     DRESS_CUDA_TRY(counted_memcpy(d_desc.get(), descs.data(), descs.size() * sizeof(ParentDesc),
                                    cudaMemcpyHostToDevice, st));
     DRESS_CUDA_TRY(counted_memcpy(d_chunks.get(), chunks.data(), chunks.size() * sizeof(Chunk),
@@ -568,6 +581,7 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
     P.need_hist = false;
     for (Prep *p : ps) P.need_hist |= p->r->want_histogram != 0;
     if (P.need_hist) DRESS_TRY(P.d_alt.alloc((size_t)values + 1, st));
+    if (staged) DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     return Status::Ok();
 }
 
@@ -618,7 +632,11 @@ Status exec_batched(BatchPlan &P, const Ctx &en)
 }
 
 // Results of the last run into the requests' host-side state.
-Status collect_batched(BatchPlan &P, const Ctx &en)
+// pre/cap (nullable): host arrays already allocated per request, with
+// their capacity in int64 words; the histograms that fit go there (their
+// ownership passes to the request, the entry is cleared).
+Status collect_batched(BatchPlan &P, const Ctx &en, std::vector<int64_t *> *pre = nullptr,
+                       const std::vector<long long> *cap = nullptr)
 {
     cudaStream_t st = en.st;
     const int nreq = (int)P.ps.size();
@@ -632,7 +650,7 @@ Status collect_batched(BatchPlan &P, const Ctx &en)
     if (P.need_hist) {
         std::vector<int64_t *> outs;
         std::vector<long long> lens;
-        DRESS_TRY(histogram_fetch(P.hist, outs, lens, &engine().pinned, st, en.num_sms));
+        DRESS_TRY(histogram_fetch(P.hist, outs, lens, en.stage, st, en.num_sms, pre, cap));
         for (int i = 0; i < nreq; ++i) {
             std::free(ps[(size_t)i]->hist_mal);
             ps[(size_t)i]->hist_mal = outs[(size_t)i];
@@ -778,12 +796,66 @@ Status capture_batched(BatchPlan &P, const Ctx &en)
     return Status::Ok();
 }
 
+// Host arrays for the histograms, allocated while the fits run.  A request's
+// histogram has at most one pair per value, and it has at most subgraphs x
+// edges values, so arrays of that size are allocated and their pages mapped
+// (a write to each page) by host threads during the device work; the fetch
+// then only copies, and trims each array to its length.  Only when the
+// bounds add up to a moderate size.
+constexpr long long PREFAULT_MIN_BYTES = 64LL << 20;
+constexpr long long PREFAULT_MAX_BYTES = 4LL << 30;
+
+struct Prefault {
+    std::vector<int64_t *> arr;
+    std::vector<long long> cap;          // int64 words
+    std::vector<std::thread> th;
+    void start(const std::vector<Prep *> &ps)
+    {
+        long long total = 0;
+        cap.assign(ps.size(), 0);
+        for (size_t i = 0; i < ps.size(); ++i)
+            if (ps[i]->r->want_histogram) {
+                cap[i] = 2 * ps[i]->items * (long long)ps[i]->E;
+                total += cap[i] * 8;
+            }
+        arr.assign(ps.size(), nullptr);
+        if (total < PREFAULT_MIN_BYTES || total > PREFAULT_MAX_BYTES) return;
+        // leave a core to the thread that drives the device
+        const int nthr = std::max(1, host_threads((long long)ps.size()) - 1);
+        for (int t = 0; t < nthr; ++t)
+            th.emplace_back([this, t, nthr] {
+                for (size_t i = (size_t)t; i < cap.size(); i += (size_t)nthr) {
+                    if (!cap[i]) continue;
+                    const size_t n = (size_t)cap[i] * sizeof(int64_t);
+                    char *a = (char *)std::malloc(n);
+                    if (a)
+                        for (size_t o = 0; o < n; o += 4096) ((volatile char *)a)[o] = 0;
+                    arr[i] = (int64_t *)a;
+                }
+            });
+    }
+    void join()
+    {
+        for (auto &t : th) t.join();
+        th.clear();
+    }
+    ~Prefault()
+    {
+        join();
+        for (int64_t *a : arr) std::free(a);
+    }
+};
+
 Status run_batched(std::vector<Prep *> &ps, const Ctx &en)
 {
     BatchPlan P;
     DRESS_TRY(plan_batched(ps, en, P));
-    DRESS_TRY(exec_batched(P, en));
-    return collect_batched(P, en);
+    Prefault pf;
+    pf.start(ps);
+    Status s = exec_batched(P, en);
+    pf.join();
+    DRESS_TRY(s);
+    return collect_batched(P, en, pf.arr.empty() ? nullptr : &pf.arr, &pf.cap);
 }
 
 Status finish(Prep &p)
@@ -815,15 +887,21 @@ Status hist_batch_core(dressx_hist_request_t *reqs, int n, bool per_fit, const C
 {
     DRESS_CUDA_TRY(cudaSetDevice(ctx.device));
     std::vector<Prep> ps((size_t)n);
-    Status first;
-    for (int i = 0; i < n; ++i) {
-        ps[(size_t)i].r = &reqs[i];
+    std::vector<Status> pst((size_t)n);
+    // requests are prepared independently, several threads for many
+    parallel_for(n, host_threads(n / 8), [&](long long ii) {
+        const size_t i = (size_t)ii;
+        ps[i].r = &reqs[i];
         reqs[i].status = DRESSX_OK;
         reqs[i].hist_flat = nullptr;
         reqs[i].hist_len = 0;
         reqs[i].multisets = nullptr;
         reqs[i].fits = 0;
-        Status s = prepare(ps[(size_t)i]);
+        pst[i] = prepare(ps[i]);
+    }, 8);
+    Status first;
+    for (int i = 0; i < n; ++i) {
+        const Status &s = pst[(size_t)i];
         if (!s.ok()) {
             reqs[i].status = s.code;
             if (first.ok()) first = s;
@@ -1056,14 +1134,19 @@ Status batch_create(dressx_hist_request_t *reqs, int n, dressx_batch_t **out)
     DRESS_CUDA_TRY(cudaSetDevice(en.device));
     dressx_batch_t *b = new dressx_batch_t();
     b->preps.resize((size_t)n);
-    for (int i = 0; i < n; ++i) {
-        Prep &p = b->preps[(size_t)i];
-        p.r = &reqs[i];
+    std::vector<Status> pst((size_t)n);
+    parallel_for(n, host_threads(n / 8), [&](long long ii) {
+        const size_t i = (size_t)ii;
+        b->preps[i].r = &reqs[i];
         reqs[i].status = DRESSX_OK;
         reqs[i].hist_flat = nullptr;
         reqs[i].hist_len = 0;
         reqs[i].multisets = nullptr;
-        Status s = prepare(p);
+        pst[i] = prepare(b->preps[i]);
+    }, 8);
+    for (int i = 0; i < n; ++i) {
+        Prep &p = b->preps[(size_t)i];
+        Status s = pst[(size_t)i];
         if (s.ok() && (p.inplace || (!p.empty && !p.batchable)))
             s = Status::Err(DRESSX_EUNSUPPORTED, "request needs the per-subgraph or in-place path");
         if (!s.ok()) {

@@ -61,6 +61,7 @@ Status Ctx::create(int dev, int sms, const dressx_config_t *config, int priority
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join2, cudaEventDisableTiming));
+    stage = new Pinned();
     return Status::Ok();
 }
 
@@ -77,6 +78,8 @@ void Ctx::destroy()
     if (side2) cudaStreamDestroy(side2);
     st = side = side2 = nullptr;
     fork = join = join2 = nullptr;
+    delete stage;
+    stage = nullptr;
 }
 
 Status Engine::init()

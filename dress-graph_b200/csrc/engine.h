@@ -104,6 +104,7 @@ struct Ctx {
     cudaStream_t side2 = nullptr;          // ... and its block items below the hubs
     cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
     const dressx_config_t *cfg = nullptr;
+    Pinned *stage = nullptr;               // host staging of this context's uploads and downloads
     // priority: CUDA stream priority of both streams (0 = default; lower
     // numbers are served first by the block scheduler)
     Status create(int dev, int sms, const dressx_config_t *config, int priority = 0);
@@ -115,7 +116,6 @@ struct Engine {
     int device = -1;
     Ctx ctx;                               // context of the legacy entry points
     std::mutex mu;                         // legacy entry points are serialised
-    Pinned pinned;
     int num_sms = 148;
     dressx_config_t cfg;
     // traffic and launch counters of the public calls (reset by the caller)

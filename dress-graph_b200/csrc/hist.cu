@@ -10,6 +10,7 @@
 // adjacent after the sort) and every NaN is a run of its own, as in the
 // reference's map.  A pass in which every segment has a single digit value
 // moves nothing and is skipped.
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -19,6 +20,7 @@
 
 #include "engine.h"
 #include "hist.h"
+#include "host_par.h"
 
 namespace dress {
 namespace {
@@ -377,7 +379,7 @@ __global__ void k_seg_ends(long long R, const int *run_seg, long long *seg_end)
 }
 
 Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
-                       cudaStream_t st, int sms)
+                       cudaStream_t st, int sms, std::vector<int64_t *> *pre, const std::vector<long long> *cap)
 {
     const int nseg = res.nseg;
     outs.assign((size_t)nseg, nullptr);
@@ -391,16 +393,6 @@ Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vecto
         R, res.run_seg.get(), d_end.get());
     std::vector<long long> end((size_t)nseg);
     DRESS_CUDA_TRY(counted_memcpy(end.data(), d_end.get(), (size_t)nseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    const size_t bytes = 2 * (size_t)R * sizeof(long long);
-    long long *host = nullptr;
-    std::vector<long long> pageable;
-    if (stage && stage->reserve(bytes).ok()) {
-        host = (long long *)stage->ptr();
-    } else {
-        pageable.resize(2 * (size_t)R);
-        host = pageable.data();
-    }
-    DRESS_CUDA_TRY(counted_memcpy(host, res.pairs.get(), bytes, cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
     // runs are grouped by segment in segment order: a segment starts where the
     // last non-empty one before it ended
@@ -413,40 +405,132 @@ Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vecto
             prev = end[(size_t)sg];
         }
     }
-    for (int sg = 0; sg < nseg; ++sg)
-        if (lens[(size_t)sg] > 0) {
-            outs[(size_t)sg] = (int64_t *)std::malloc((size_t)lens[(size_t)sg] * sizeof(int64_t));
-            if (!outs[(size_t)sg]) {
-                for (auto &o : outs) std::free(o);
-                outs.assign((size_t)nseg, nullptr);
-                return Status::Err(DRESSX_ENOMEM, "host allocation of the histograms failed");
-            }
-        }
-    // copy out, several threads for large results
-    auto copy_range = [&](int a, int b) {
-        for (int sg = a; sg < b; ++sg)
-            if (lens[(size_t)sg] > 0)
-                std::memcpy(outs[(size_t)sg], host + 2 * first[(size_t)sg], (size_t)lens[(size_t)sg] * sizeof(int64_t));
-    };
-    const int nthr = bytes > (64u << 20) ? 8 : 1;
-    if (nthr == 1 || nseg < 2) {
-        copy_range(0, nseg);
+    const size_t bytes = 2 * (size_t)R * sizeof(long long);
+    long long *host = nullptr;
+    std::vector<long long> pageable;
+    const bool pinned = stage && stage->reserve(bytes).ok();
+    if (pinned) {
+        host = (long long *)stage->ptr();
     } else {
-        // split by bytes so the threads copy about the same amount
-        std::vector<int> cut(1, 0);
+        pageable.resize(2 * (size_t)R);
+        host = pageable.data();
+    }
+    // Large results: one part per host thread, balanced by bytes.  Each part
+    // is its own download; while the parts stream in, the threads allocate
+    // their segments' arrays and touch every page (the page faults of fresh
+    // memory cost more than the copy), then copy their part once it landed.
+    const int nthr = pinned && bytes > (64u << 20) && nseg > 1 ? host_threads(nseg) : 1;
+    std::vector<int> cut(1, 0);
+    {
         const long long per = (2 * R + nthr - 1) / nthr;
         long long acc = 0;
         for (int sg = 0; sg < nseg; ++sg) {
             acc += lens[(size_t)sg];
             if (acc >= per * (long long)cut.size() && (int)cut.size() < nthr) cut.push_back(sg + 1);
         }
-        cut.push_back(nseg);
-        std::vector<std::thread> th;
-        for (size_t t = 0; t + 1 < cut.size(); ++t)
-            if (cut[t + 1] > cut[t]) th.emplace_back(copy_range, cut[t], cut[t + 1]);
-        for (auto &t : th) t.join();
+        if (cut.back() != nseg) cut.push_back(nseg);
     }
-    return Status::Ok();
+    const int parts = (int)cut.size() - 1;
+    std::vector<cudaEvent_t> ev((size_t)parts, nullptr);
+    Status err;
+    for (int t = 0; t < parts && err.ok(); ++t) {
+        // the part's runs: from the first run of its first segment to the
+        // end of its last non-empty segment
+        long long r0 = -1, r1 = -1;
+        for (int sg = cut[(size_t)t]; sg < cut[(size_t)t + 1]; ++sg)
+            if (lens[(size_t)sg] > 0) {
+                if (r0 < 0) r0 = first[(size_t)sg];
+                r1 = end[(size_t)sg];
+            }
+        if (r0 < 0) continue;
+        if (cudaEventCreateWithFlags(&ev[(size_t)t], cudaEventDisableTiming) != cudaSuccess) {
+            ev[(size_t)t] = nullptr;
+            err = Status::Err(DRESSX_ECUDA, "event creation failed");
+            break;
+        }
+        cudaError_t e = counted_memcpy(host + 2 * r0, res.pairs.get() + 2 * r0, 2 * (size_t)(r1 - r0) * sizeof(long long),
+                                       cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[(size_t)t], st);
+        if (e != cudaSuccess) err = Status::Err(DRESSX_ECUDA, std::string("histogram download: ") + cudaGetErrorString(e));
+    }
+    // ready: parts whose download is complete (or -1 once the downloads failed)
+    std::vector<char> given((size_t)nseg, 0);    // segments that took a given array
+    std::atomic<int> ready{0};
+    std::atomic<bool> nomem{false};
+    // A part's thread maps the pages of its arrays (a write to each page) while
+    // the part's download is in flight, and once it landed copies into the
+    // arrays mapped so far and then into fresh ones, whose page faults the
+    // copy takes itself.
+    auto part_work = [&](int t) {
+        const int s0 = cut[(size_t)t], s1 = cut[(size_t)t + 1];
+        // a segment's array: the one given for it when it fits (true), else a new one
+        auto alloc = [&](int sg) {
+            const size_t n = (size_t)lens[(size_t)sg] * sizeof(int64_t);
+            if (n && pre && (*pre)[(size_t)sg] && lens[(size_t)sg] <= (*cap)[(size_t)sg]) {
+                outs[(size_t)sg] = (*pre)[(size_t)sg];
+                (*pre)[(size_t)sg] = nullptr;
+                given[(size_t)sg] = 1;
+                return true;
+            }
+            char *a = n ? (char *)std::malloc(n) : nullptr;
+            outs[(size_t)sg] = (int64_t *)a;
+            if (n && !a) nomem = true;
+            return false;
+        };
+        auto copy = [&](int sg) {
+            int64_t *a = outs[(size_t)sg];
+            if (!a) return;
+            const size_t n = (size_t)lens[(size_t)sg] * sizeof(int64_t);
+            std::memcpy(a, host + 2 * first[(size_t)sg], n);
+            if (given[(size_t)sg] && lens[(size_t)sg] < (*cap)[(size_t)sg]) {
+                // trim a given array (shrinking keeps the data)
+                void *r2 = std::realloc(a, n);
+                if (r2) outs[(size_t)sg] = (int64_t *)r2;
+            }
+        };
+        int sg = s0;
+        int r;
+        while ((r = ready.load()) >= 0 && r <= t) {
+            if (sg == s1) {
+                std::this_thread::yield();
+                continue;
+            }
+            if (!alloc(sg)) {
+                char *a = (char *)outs[(size_t)sg];
+                const size_t n = (size_t)lens[(size_t)sg] * sizeof(int64_t);
+                if (a)
+                    for (size_t o = 0; o < n; o += 4096) ((volatile char *)a)[o] = 0;
+            }
+            ++sg;
+        }
+        if (r < 0) return;
+        for (int q = s0; q < sg; ++q) copy(q);
+        for (int q = sg; q < s1; ++q) {
+            alloc(q);
+            copy(q);
+        }
+    };
+    std::vector<std::thread> th;
+    if (parts > 1)
+        for (int t = 0; t < parts; ++t) th.emplace_back(part_work, t);
+    // this thread waits for the downloads in order and releases the parts
+    for (int t = 0; t < parts && err.ok(); ++t) {
+        if (ev[(size_t)t] && cudaEventSynchronize(ev[(size_t)t]) != cudaSuccess)
+            err = Status::Err(DRESSX_ECUDA, "histogram download failed");
+        else
+            ready = t + 1;
+    }
+    if (!err.ok()) ready = -1;
+    if (err.ok() && parts == 1) part_work(0);
+    for (auto &t : th) t.join();
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    if (err.ok() && nomem) err = Status::Err(DRESSX_ENOMEM, "host allocation of the histograms failed");
+    if (!err.ok()) {
+        for (auto &o : outs) std::free(o);
+        outs.assign((size_t)nseg, nullptr);
+    }
+    return err;
 }
 
 Status histogram_download(HistResult &res, std::vector<std::vector<long long>> &out, cudaStream_t st)

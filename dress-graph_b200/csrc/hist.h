@@ -21,9 +21,13 @@ Status histogram_device(unsigned long long *keys, unsigned long long *alt, const
 Status histogram_download(HistResult &res, std::vector<std::vector<long long>> &out, cudaStream_t st);
 // Same results straight into malloc'd per-segment arrays (outs[s], lens[s]
 // int64 entries; NULL and 0 for an empty segment; the caller frees them),
-// through the pinned staging buffer when one is given.
+// through the pinned staging buffer when one is given.  pre/cap (nullable):
+// malloc'd arrays that already exist per segment and their capacity in
+// int64 entries; a segment that fits takes its array (trimmed to length,
+// the entry cleared), the others get new ones.
 Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
-                       cudaStream_t st, int sms);
+                       cudaStream_t st, int sms, std::vector<int64_t *> *pre = nullptr,
+                       const std::vector<long long> *cap = nullptr);
 
 // Stable ascending sort of n unsigned 64-bit keys with a 32-bit payload
 // (LSD radix, 8-bit digits; digits equal on every key are skipped).  The

@@ -8,7 +8,6 @@ Same entry points, argument names, defaults and result fields as
 many graphs' histograms in one persistent launch.
 """
 import ctypes
-import weakref
 from dataclasses import dataclass, field
 from typing import List, Optional, Tuple
 
@@ -58,18 +57,49 @@ def _malloc_copy(arr, ctype):
     return ctypes.cast(raw, ctypes.POINTER(ctype))
 
 
+class _Block:
+    """A malloc'd int64 array handed over by the library: numpy reads it in
+    place through the array interface, and the block is released with
+    dressx_free when the last array over it goes away."""
+
+    __slots__ = ("addr", "n", "free")
+
+    def __init__(self, addr, n, free):
+        self.addr, self.n, self.free = addr, n, free
+
+    @property
+    def __array_interface__(self):
+        return {"shape": (self.n,), "typestr": "<i8", "data": (self.addr, False), "version": 3}
+
+    def __del__(self):
+        self.free(self.addr)
+
+
 def _take_i64(ptr, n):
     """A malloc'd int64 array from the library as numpy, without a copy; the
     memory is released with dressx_free once no array refers to it."""
     if not ptr:
         return np.zeros(0, dtype=np.int64)
-    addr = ctypes.cast(ptr, ctypes.c_void_p).value
+    addr = ptr if isinstance(ptr, int) else ctypes.cast(ptr, ctypes.c_void_p).value
     if n <= 0:
         lib().dressx_free(addr)
         return np.zeros(0, dtype=np.int64)
-    buf = (ctypes.c_int64 * int(n)).from_address(addr)
-    weakref.finalize(buf, lib().dressx_free, addr)
-    return np.frombuffer(buf, dtype=np.int64)
+    return np.asarray(_Block(addr, int(n), lib().dressx_free))
+
+
+def _request_view(reqs):
+    """The request array as a numpy record array over the same memory, for
+    filling and reading many requests at once."""
+    T = _abi.HistRequest
+    ptr_fields = {"graph", "hist_flat", "multisets"}
+    names, formats, offsets = [], [], []
+    for name, ctype in T._fields_:
+        names.append(name)
+        formats.append(np.uintp if name in ptr_fields else np.dtype(ctype))
+        offsets.append(getattr(T, name).offset)
+    dt = np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": ctypes.sizeof(T)})
+    raw = (ctypes.c_char * ctypes.sizeof(reqs)).from_buffer(reqs)
+    return np.frombuffer(raw, dtype=dt)
 
 
 def _arr(ptr, n, dtype):
@@ -250,31 +280,32 @@ def hist_requests(graphs, kind, k, max_iterations=100, epsilon=1e-6, n_samples=0
     num_subgraphs, fits)."""
     n = len(graphs)
     reqs = (_abi.HistRequest * n)()
-    for i, g in enumerate(graphs):
-        r = reqs[i]
-        r.graph = g.ptr
-        r.kind = int(kind)
-        r.k = int(k)
-        r.max_iterations = int(max_iterations)
-        r.epsilon = float(epsilon)
-        r.n_samples = int(n_samples)
-        r.seed = int(seed) & 0xFFFFFFFF
-        r.offset = int(offset)
-        r.stride = int(stride)
-        r.want_histogram = 1 if compute_histogram else 0
-        r.keep_multisets = 1 if keep_multisets else 0
+    v = _request_view(reqs)
+    v["graph"] = [ctypes.cast(g.ptr, ctypes.c_void_p).value for g in graphs]
+    v["kind"] = int(kind)
+    v["k"] = int(k)
+    v["max_iterations"] = int(max_iterations)
+    v["epsilon"] = float(epsilon)
+    v["n_samples"] = int(n_samples)
+    v["seed"] = int(seed) & 0xFFFFFFFF
+    v["offset"] = int(offset)
+    v["stride"] = int(stride)
+    v["want_histogram"] = 1 if compute_histogram else 0
+    v["keep_multisets"] = 1 if keep_multisets else 0
     fn = lib().dressx_hist_batch_per_fit if per_fit else lib().dressx_hist_batch
     code = fn(reqs, n)
+    flats, lens = v["hist_flat"].tolist(), v["hist_len"].tolist()
+    mss, nsub = v["multisets"].tolist(), v["num_subgraphs"].tolist()
+    fits, status = v["fits"].tolist(), v["status"].tolist()
+    v["hist_flat"] = 0
     out = []
     for i, g in enumerate(graphs):
-        r = reqs[i]
-        flat = _take_i64(r.hist_flat, r.hist_len)
-        r.hist_flat = None
         ms = None
-        if r.multisets:
-            ms = _arr(r.multisets, r.num_subgraphs * g.E, np.float64).reshape(r.num_subgraphs, g.E)
-            lib().dressx_free(ctypes.cast(r.multisets, ctypes.c_void_p))
-        out.append((flat, ms, r.num_subgraphs, r.fits, r.status))
+        if mss[i]:
+            ms = _arr(ctypes.cast(mss[i], ctypes.POINTER(ctypes.c_double)), nsub[i] * g.E,
+                      np.float64).reshape(nsub[i], g.E)
+            lib().dressx_free(mss[i])
+        out.append((_take_i64(flats[i], lens[i]), ms, nsub[i], fits[i], status[i]))
     _check(code)
     return out
 
