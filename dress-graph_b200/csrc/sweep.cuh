@@ -219,31 +219,19 @@ struct KbnStream {
     }
 };
 
-// Same over an ascending run in global memory: the self term's rank by
-// binary search, then 32-term windows, the next window's loads in flight
-// while the current one is summed, so the chain does not wait on L2 or HBM.
-__device__ __forceinline__ double kbn_merge_stream(const double *__restrict__ a, int n, double x)
+// KBN steps over a[b..e) in index order, in W-term windows: the next
+// window's loads are in flight while the current one is summed, and the
+// ragged tail is loaded at once, so the chain does not wait on L2 or HBM
+// term by term.
+__device__ __forceinline__ void kbn_run(const double *__restrict__ a, int b, int e, double &s, double &c)
 {
     constexpr int W = 32;
-    int lo = 0, hi = n;                      // first index with a[idx] >= x
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (a[mid] < x) lo = mid + 1;
-        else hi = mid;
-    }
-    const int pos = lo;
-    // s = -0.0, c = +0.0: the first step then leaves s = that term, c = +0.0
-    // exactly, as starting the sum at it does (for every finite term, zeros
-    // of either sign included)
-    double s = -0.0, c = 0.0;
-    int i = 0;
-    for (; i < pos; ++i) kbn_step(s, c, a[i]);
-    kbn_step(s, c, x);
-    if (i + W <= n) {
+    int i = b;
+    if (i + W <= e) {
         double cur[W], nxt[W];
 #pragma unroll
         for (int t = 0; t < W; ++t) cur[t] = a[i + t];
-        while (i + 2 * W <= n) {
+        while (i + 2 * W <= e) {
 #pragma unroll
             for (int t = 0; t < W; ++t) nxt[t] = a[i + W + t];
 #pragma unroll
@@ -256,14 +244,43 @@ __device__ __forceinline__ double kbn_merge_stream(const double *__restrict__ a,
         for (int t = 0; t < W; ++t) kbn_step(s, c, cur[t]);
         i += W;
     }
-    for (; i < n; ++i) kbn_step(s, c, a[i]);
+    if (i < e) {
+        double tail[W];
+#pragma unroll
+        for (int t = 0; t < W; ++t) tail[t] = i + t < e ? a[i + t] : 0.0;
+#pragma unroll
+        for (int t = 0; t < W; ++t)
+            if (i + t < e) kbn_step(s, c, tail[t]);
+    }
+}
+
+// Same over an ascending run in global memory: the self term's rank by
+// binary search, then the windowed steps before it, the self term, and the
+// windowed steps after it.
+__device__ __forceinline__ double kbn_merge_stream(const double *__restrict__ a, int n, double x)
+{
+    int lo = 0, hi = n;                      // first index with a[idx] >= x
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    const int pos = lo;
+    // s = -0.0, c = +0.0: the first step then leaves s = that term, c = +0.0
+    // exactly, as starting the sum at it does (for every finite term, zeros
+    // of either sign included)
+    double s = -0.0, c = 0.0;
+    kbn_run(a, 0, pos, s, c);
+    kbn_step(s, c, x);
+    kbn_run(a, pos, n, s, c);
     return dadd(s, c);
 }
 
 // Sorted KBN of the n terms term(0..n) taken in stored order, with x merged
-// at its rank, while checking that the terms ascend; false when they do not
-// (the sum is then unusable).  Windows of W terms, the next window gathered
-// while the current one is summed; x is looked for once per window.
+// at its rank, while checking that the terms ascend; false, without
+// finishing, at the first window that does not ascend.  Windows of W terms,
+// the next window gathered while the current one is summed; x is looked for
+// once per window; the ragged tail is gathered at once.
 template <int W, class Term>
 __device__ __forceinline__ bool kbn_stream_checked(int n, double x, Term term, double &out)
 {
@@ -283,7 +300,7 @@ __device__ __forceinline__ bool kbn_stream_checked(int n, double x, Term term, d
             bool o = !(cur[0] < prev);
 #pragma unroll
             for (int t = 0; t + 1 < W; ++t) o &= !(cur[t + 1] < cur[t]);
-            ok &= o;
+            if (!o) return false;        // out of order: the item is sorted and summed elsewhere
             prev = cur[W - 1];
             if (!ins && !(cur[W - 1] < x)) {
 #pragma unroll
@@ -304,19 +321,31 @@ __device__ __forceinline__ bool kbn_stream_checked(int n, double x, Term term, d
             for (int t = 0; t < W; ++t) cur[t] = nxt[t];
         }
     }
-    for (; i < n; ++i) {
-        const double v = term(i);
-        ok &= !(v < prev);
-        prev = v;
-        if (!ins && !(v < x)) {
-            kbn_step(s, c, x);
-            ins = true;
-        }
-        kbn_step(s, c, v);
+    if (i < n) {
+        // the ragged tail, its terms loaded at once
+        double tail[W];
+#pragma unroll
+        for (int t = 0; t < W; ++t) tail[t] = i + t < n ? term(i + t) : 0.0;
+#pragma unroll
+        for (int t = 0; t < W; ++t)
+            if (i + t < n) {
+                ok &= !(tail[t] < prev);
+                prev = tail[t];
+            }
+        if (!ok) return false;
+#pragma unroll
+        for (int t = 0; t < W; ++t)
+            if (i + t < n) {
+                if (!ins && !(tail[t] < x)) {
+                    kbn_step(s, c, x);
+                    ins = true;
+                }
+                kbn_step(s, c, tail[t]);
+            }
     }
     if (!ins) kbn_step(s, c, x);
     out = dadd(s, c);
-    return ok;
+    return true;
 }
 
 // Same over an ascending buffer (one thread).
