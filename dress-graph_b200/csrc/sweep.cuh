@@ -584,37 +584,168 @@ __global__ void __launch_bounds__(256) k_edge_med(Sweep s, int begin, int end)
     block_max_to(max_slot(s), delta);
 }
 
-// one warp per queued item: restore ascending order, write it back, and sum
-// the sorted terms (lane 0) -- queued items are the minority
+// ---- packed warp sort of one queued streamed item --------------------------------------
+// The terms are sorted as 64-bit words: the term's order-preserving bits with
+// the low IDX_BITS replaced by its stored position, the replaced bits kept
+// beside it (lo, by position).  Words are distinct, so the sort is total, and
+// moving a word moves key and position together: no payload array in shared
+// memory, half the traffic of sorting keys with a payload, and more warps
+// per SM.  Afterwards the payload (slot edge id or pair) is gathered by
+// position.  Terms equal in all but their low IDX_BITS come out in stored
+// order, so the order of the full values is checked and, where such a near
+// tie is inverted (rare), repaired.
+constexpr int IDX_BITS = 9;
+constexpr unsigned long long IDX_MASK = (1ULL << IDX_BITS) - 1;
+static_assert(MED_CAP <= (1 << IDX_BITS), "positions must fit the index bits");
+
+// order-preserving map of a double to 64 unsigned bits, and back
+__device__ __forceinline__ unsigned long long ord_bits(double x)
+{
+    const unsigned long long u = (unsigned long long)__double_as_longlong(x);
+    return u ^ ((u >> 63) ? ~0ULL : 0x8000000000000000ULL);
+}
+__device__ __forceinline__ double from_ord(unsigned long long k)
+{
+    return __longlong_as_double((long long)(k ^ ((k >> 63) ? 0x8000000000000000ULL : ~0ULL)));
+}
+
+__device__ __forceinline__ void pack_term(unsigned long long *wb, unsigned short *lo, int k, double v)
+{
+    const unsigned long long b = ord_bits(v);
+    wb[k] = (b & ~IDX_MASK) | (unsigned long long)k;
+    lo[k] = (unsigned short)(b & IDX_MASK);
+}
+
+// warp bitonic sort of w[0..n), the network of sort_shared
+__device__ __forceinline__ void sort_words(unsigned long long *w, int n, int lane)
+{
+    int M = 1;
+    while (M < n) M <<= 1;
+    for (int k = 2; k <= M; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int q = lane; q < (M >> 1); q += 32) {
+                const int i = ((q & ~(j - 1)) << 1) | (q & (j - 1));
+                const int p = (j == (k >> 1)) ? (i ^ (k - 1)) : (i | j);
+                const int a = i < p ? i : p, b = i < p ? p : i;
+                if (b < n) {
+                    const unsigned long long x = w[a], y = w[b];
+                    if (y < x) {
+                        w[a] = y;
+                        w[b] = x;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Ascending order of w[0..n): odd-even transposition passes while they last
+// at most MAX_PASSES (nearly sorted input), else the bitonic sort.
+__device__ __forceinline__ void fix_words(unsigned long long *w, int n, int lane)
+{
+    int d = 0;
+    for (int k = lane; k + 1 < n; k += 32) d += w[k + 1] < w[k];
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    if (!far_from_sorted(d, n)) {
+        for (int pass = 0; pass < MAX_PASSES; ++pass) {
+            bool sw = false;
+            for (int parity = 0; parity < 2; ++parity) {
+                for (int i = 2 * lane + parity; i + 1 < n; i += 64) {
+                    const unsigned long long x = w[i], y = w[i + 1];
+                    if (y < x) {
+                        w[i] = y;
+                        w[i + 1] = x;
+                        sw = true;
+                    }
+                }
+                __syncwarp();
+            }
+            if (!__any_sync(0xffffffffu, sw)) return;
+        }
+    }
+    sort_words(w, n, lane);
+}
+
+// Sorted words back to terms: the sorted values to out[0..n), the payload
+// pay[0..n) (global, in stored order) permuted to the sorted order in place,
+// parked in out on the way (every read of pay precedes every write).
+template <class P>
+__device__ __forceinline__ long long payload_bits(P v)
+{
+    long long b = 0;
+    memcpy(&b, &v, sizeof(P));
+    return b;
+}
+template <class P>
+__device__ __forceinline__ P payload_of(long long b)
+{
+    P v;
+    memcpy(&v, &b, sizeof(P));
+    return v;
+}
+
+template <class P>
+__device__ __forceinline__ void place_sorted(unsigned long long *wb, const unsigned short *lo, int n, int lane,
+                                             P *pay, double *out)
+{
+    static_assert(sizeof(P) <= sizeof(double), "payload parks in a value slot");
+    for (int k = lane; k < n; k += 32)
+        out[k] = __longlong_as_double(payload_bits(pay[(int)(wb[k] & IDX_MASK)]));
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) {
+        const unsigned long long w = wb[k];
+        const unsigned long long full = (w & ~IDX_MASK) | lo[(int)(w & IDX_MASK)];
+        pay[k] = payload_of<P>(__double_as_longlong(out[k]));
+        out[k] = from_ord(full);
+        wb[k] = full;
+    }
+    __syncwarp();
+    bool desc = false;
+    for (int k = lane; k + 1 < n; k += 32) desc |= wb[k + 1] < wb[k];
+    if (__any_sync(0xffffffffu, desc)) {
+        // an inverted near tie: insertion by the full value, one lane
+        if (lane == 0) {
+            for (int k = 1; k < n; ++k) {
+                const unsigned long long key = wb[k];
+                const P pk = pay[k];
+                int m = k - 1;
+                while (m >= 0 && key < wb[m]) {
+                    wb[m + 1] = wb[m];
+                    pay[m + 1] = pay[m];
+                    --m;
+                }
+                wb[m + 1] = key;
+                pay[m + 1] = pk;
+            }
+            for (int k = 0; k < n; ++k) out[k] = from_ord(wb[k]);
+        }
+        __syncwarp();
+    }
+}
+
+// one warp per queued item: restore ascending order, write it back with the
+// sorted terms; the sums follow (k_*_med_sum) -- queued items are the minority
 template <bool UNIF>
 __global__ void __launch_bounds__(256) k_vertex_med_sort(Sweep s)
 {
     extern __shared__ __align__(16) unsigned char smw[];
     if (skipped(s)) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    double *kb = (double *)smw + (size_t)wid * MED_CAP;
-    int *pb = (int *)((double *)smw + (size_t)nwarps * MED_CAP) + (size_t)wid * MED_CAP;
+    unsigned long long *wb = (unsigned long long *)smw + (size_t)wid * MED_CAP;
+    unsigned short *lo = (unsigned short *)((unsigned long long *)smw + (size_t)nwarps * MED_CAP) +
+                         (size_t)wid * MED_CAP;
     const int n_items = (int)s.qcount[0];
     for (int q = blockIdx.x * nwarps + wid; q < n_items; q += gridDim.x * nwarps) {
         const int i = s.qv[q];
         const long long b = s.row_off[i];
         const int deg = (int)(s.row_off[i + 1] - b);
-        for (int k = lane; k < deg; k += 32) {
-            int e = s.row_eid[b + k];
-            pb[k] = e;
-            kb[k] = prod<UNIF>(s, e);
-        }
+        int *rows = s.row_eid + b;
+#pragma unroll 4
+        for (int k = lane; k < deg; k += 32) pack_term(wb, lo, k, prod<UNIF>(s, rows[k]));
         __syncwarp();
-        int d = 0;
-        for (int k = lane; k + 1 < deg; k += 32) d += kb[k + 1] < kb[k];
-        for (int o2 = 16; o2 > 0; o2 >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o2);
-        fix_order(kb, pb, deg, lane, 32, WarpSync(), WarpAny(), far_from_sorted(d, deg));
-        double *out = s.skey + (b - s.sbase);
-        for (int k = lane; k < deg; k += 32) {
-            s.row_eid[b + k] = pb[k];
-            out[k] = kb[k];
-        }
-        __syncwarp();
+        fix_words(wb, deg, lane);
+        place_sorted(wb, lo, deg, lane, rows, s.skey + (b - s.sbase));
     }
 }
 
@@ -624,29 +755,23 @@ __global__ void __launch_bounds__(256) k_edge_med_sort(Sweep s)
     extern __shared__ __align__(16) unsigned char smw[];
     if (skipped(s)) return;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    double *kb = (double *)smw + (size_t)wid * MED_CAP;
-    int2 *pb = (int2 *)((double *)smw + (size_t)nwarps * MED_CAP) + (size_t)wid * MED_CAP;
+    unsigned long long *wb = (unsigned long long *)smw + (size_t)wid * MED_CAP;
+    unsigned short *lo = (unsigned short *)((unsigned long long *)smw + (size_t)nwarps * MED_CAP) +
+                         (size_t)wid * MED_CAP;
     const int n_items = (int)s.qcount[1];
     for (int q = blockIdx.x * nwarps + wid; q < n_items; q += gridDim.x * nwarps) {
         const int j = s.qe[q];
         const long long o = s.ioff[j];
         const int nc = (int)(s.ioff[j + 1] - o);
+        int2 *prs = s.pairs + o;
+#pragma unroll 4
         for (int k = lane; k < nc; k += 32) {
-            int2 pr = s.pairs[o + k];
-            pb[k] = pr;
-            kb[k] = dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y));
+            const int2 pr = prs[k];
+            pack_term(wb, lo, k, dadd(prod<UNIF>(s, pr.x), prod<UNIF>(s, pr.y)));
         }
         __syncwarp();
-        int d = 0;
-        for (int k = lane; k + 1 < nc; k += 32) d += kb[k + 1] < kb[k];
-        for (int o2 = 16; o2 > 0; o2 >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o2);
-        fix_order(kb, pb, nc, lane, 32, WarpSync(), WarpAny(), far_from_sorted(d, nc));
-        double *out = s.tkey + (o - s.tbase);
-        for (int k = lane; k < nc; k += 32) {
-            s.pairs[o + k] = pb[k];
-            out[k] = kb[k];
-        }
-        __syncwarp();
+        fix_words(wb, nc, lane);
+        place_sorted(wb, lo, nc, lane, prs, s.tkey + (o - s.tbase));
     }
 }
 
@@ -838,6 +963,11 @@ struct LaunchCfg {
 
 constexpr int THR = 128;
 constexpr int MED_THR = 256;
+// The packed sort uses 10 bytes of shared memory per term (word + low bits).
+// The launches ask for 12 (vertices) and 16 (edges), which holds them to 4
+// and 3 CTAs per SM: measured on the 28M-edge power-law fit, letting them
+// fill the SMs crowds out the block-bin kernels running concurrently on the
+// side streams, and the sweep takes 6 % longer.
 inline size_t med_smem_vertex() { return (size_t)(MED_THR / 32) * MED_CAP * (8 + 4); }
 inline size_t med_smem_edge() { return (size_t)(MED_THR / 32) * MED_CAP * (8 + 8); }
 
