@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <climits>
 #include <chrono>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -740,7 +741,23 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
             if (m < epsilon) { conv = it; break; }
         }
         done = hi;
-        if (chunk < MAX_CHUNK) chunk *= 2;
+        // Next chunk: the sweeps that the decay of the last three deltas
+        // predicts until the tolerance, plus two, when they decay; else twice
+        // the last chunk.  Sweeps past convergence return at once but still
+        // cost their launches (≈ 3 µs each), a short chunk costs one more
+        // host round trip.
+        int next = chunk < MAX_CHUNK ? 2 * chunk : MAX_CHUNK;
+        if (conv < 0 && done >= 4) {
+            double m1, m0;
+            std::memcpy(&m1, &hmax[(done - 1) % RING], sizeof(m1));
+            std::memcpy(&m0, &hmax[(done - 4) % RING], sizeof(m0));
+            if (m1 >= epsilon && m1 > 0.0 && m0 > m1) {
+                const double rate = std::pow(m1 / m0, 1.0 / 3.0);
+                const double need = std::log(epsilon / m1) / std::log(rate);
+                if (need >= 0.0 && need < (double)MAX_CHUNK) next = std::max(2, (int)std::ceil(need) + 2);
+            }
+        }
+        chunk = std::min(MAX_CHUNK, (next + 1) & ~1);
     }
     const int last = conv >= 0 ? conv : max_iterations - 1;
     // device time of the sweeps (the chunk tails after convergence return at once)

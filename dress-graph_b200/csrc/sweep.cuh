@@ -276,6 +276,79 @@ __device__ __forceinline__ double kbn_merge_stream(const double *__restrict__ a,
     return dadd(s, c);
 }
 
+// ---- asynchronous global -> shared copies (cp.async, 8 bytes a thread) ----------------
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Same as kbn_merge_stream for one long run, by a whole warp: the lanes copy
+// chunks of HUB_CHUNK terms into shared memory (buf, 2 x HUB_CHUNK doubles)
+// one chunk ahead of lane 0, which runs the serial chain from shared memory.
+// The result is valid in lane 0.
+constexpr int HUB_CHUNK = 1024;
+constexpr size_t HUB_SMEM = 2 * HUB_CHUNK * sizeof(double);
+__device__ __forceinline__ double kbn_merge_stream_warp(const double *__restrict__ a, int n, double x, double *buf,
+                                                        int lane)
+{
+    int pos = 0;
+    if (lane == 0) {
+        int lo = 0, hi = n;                  // first index with a[idx] >= x
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (a[mid] < x) lo = mid + 1;
+            else hi = mid;
+        }
+        pos = lo;
+    }
+    pos = __shfl_sync(0xffffffffu, pos, 0);
+    const int nch = (n + HUB_CHUNK - 1) / HUB_CHUNK;
+    auto issue = [&](int ch) {
+        if (ch < nch) {
+            const int base = ch * HUB_CHUNK;
+            double *dst = buf + (ch & 1) * HUB_CHUNK;
+            for (int t = lane; t < HUB_CHUNK && base + t < n; t += 32) cp_async8(dst + t, a + base + t);
+        }
+        cp_async_commit();                   // one group per chunk on every lane, empty or not
+    };
+    double s = -0.0, c = 0.0;                // see kbn_merge_stream
+    issue(0);
+    for (int ch = 0; ch < nch; ++ch) {
+        issue(ch + 1);
+        cp_async_wait_one();                 // this lane's copies of chunk ch landed ...
+        __syncwarp();                        // ... and every lane's
+        if (lane == 0) {
+            const double *src = buf + (ch & 1) * HUB_CHUNK;
+            const int base = ch * HUB_CHUNK, cnt = min(HUB_CHUNK, n - base);
+            const int cut = min(max(pos - base, 0), cnt);     // terms of this chunk before x
+            int t = 0;
+            for (; t + 8 <= cut; t += 8) {
+                double v[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) v[q] = src[t + q];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) kbn_step(s, c, v[q]);
+            }
+            for (; t < cut; ++t) kbn_step(s, c, src[t]);
+            if (pos >= base && pos < base + cnt) kbn_step(s, c, x);
+            for (; t + 8 <= cnt; t += 8) {
+                double v[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) v[q] = src[t + q];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) kbn_step(s, c, v[q]);
+            }
+            for (; t < cnt; ++t) kbn_step(s, c, src[t]);
+        }
+        __syncwarp();                        // chunk ch read before its buffer is refilled
+    }
+    if (pos == n) kbn_step(s, c, x);
+    return dadd(s, c);
+}
+
 // Sorted KBN of the n terms term(0..n) taken in stored order, with x merged
 // at its rank, while checking that the terms ascend; false, without
 // finishing, at the first window that does not ascend.  Windows of W terms,
@@ -902,11 +975,17 @@ __global__ void __launch_bounds__(512) k_edge_block(Sweep s, int begin, int end,
 template <bool UNIF>
 __global__ void __launch_bounds__(32) k_vertex_block_sum(Sweep s, int big0, int nbig, int blk0, int nblk)
 {
+    extern __shared__ __align__(16) unsigned char smw[];
     if (skipped(s)) return;
     int i;
     if ((int)blockIdx.x < nbig) {
-        if (threadIdx.x) return;
+        // a hub row: the whole warp streams its terms
         i = big0 + (int)blockIdx.x;
+        const int deg = (int)(s.row_off[i + 1] - s.row_off[i]);
+        const double v = kbn_merge_stream_warp(s.bkey_v + s.bofs_v[i - s.bv0], deg, four_nw(s, i), (double *)smw,
+                                               (int)threadIdx.x);
+        if (threadIdx.x == 0) s.vd[i] = dsqrt(v);
+        return;
     } else {
         const int t = ((int)blockIdx.x - nbig) * 32 + (int)threadIdx.x;
         if (t >= nblk) return;
@@ -919,16 +998,23 @@ __global__ void __launch_bounds__(32) k_vertex_block_sum(Sweep s, int big0, int 
 template <bool UNIF>
 __global__ void __launch_bounds__(32) k_edge_block_sum(Sweep s, int big0, int nbig, int blk0, int nblk)
 {
+    extern __shared__ __align__(16) unsigned char smw[];
     if (skipped(s)) return;
     int j = -1;
-    if ((int)blockIdx.x < nbig) {
-        if (threadIdx.x == 0) j = big0 + (int)blockIdx.x;
-    } else {
+    if ((int)blockIdx.x >= nbig) {
         const int t = ((int)blockIdx.x - nbig) * 32 + (int)threadIdx.x;
         if (t < nblk) j = blk0 + t;
     }
     double delta = 0.0;
-    if (j >= 0) {
+    if ((int)blockIdx.x < nbig) {
+        // a hub edge: the whole warp streams its terms
+        j = big0 + (int)blockIdx.x;
+        const int u = s.eu[j], v = s.ev[j];
+        const int nc = (int)(s.ioff[j + 1] - s.ioff[j]);
+        const double sum = kbn_merge_stream_warp(s.bkey_e + s.bofs_e[j - s.be0], nc, self_term<UNIF>(s, j, u, v),
+                                                 (double *)smw, (int)threadIdx.x);
+        if (threadIdx.x == 0) delta = finish_edge<UNIF>(s, j, u, v, sum);
+    } else if (j >= 0) {
         const int u = s.eu[j], v = s.ev[j];
         const int nc = (int)(s.ioff[j + 1] - s.ioff[j]);
         delta = finish_edge<UNIF>(s, j, u, v, kbn_merge_stream(s.bkey_e + s.bofs_e[j - s.be0], nc,
@@ -997,11 +1083,11 @@ void launch_blocks(const Sweep &s, const Bins &b, const LaunchCfg &c)
         if (EDGE) {
             count_launch(), k_edge_block<UNIF, false><<<grid_for(nbig, 1, c.sms), 512, (size_t)c.block_cap * 16,
                                                   c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.block_cap);
-            count_launch(), k_edge_block_sum<UNIF><<<nbig, 32, 0, c.side>>>(s, b.start[BBIG], nbig, 0, 0);
+            count_launch(), k_edge_block_sum<UNIF><<<nbig, 32, HUB_SMEM, c.side>>>(s, b.start[BBIG], nbig, 0, 0);
         } else {
             count_launch(), k_vertex_block<UNIF, false><<<grid_for(nbig, 1, c.sms), 512, (size_t)c.vblock_cap * 12,
                                                     c.side>>>(s, b.start[BBIG], b.start[BBIG + 1], c.vblock_cap);
-            count_launch(), k_vertex_block_sum<UNIF><<<nbig, 32, 0, c.side>>>(s, b.start[BBIG], nbig, 0, 0);
+            count_launch(), k_vertex_block_sum<UNIF><<<nbig, 32, HUB_SMEM, c.side>>>(s, b.start[BBIG], nbig, 0, 0);
         }
     }
     if (nblk > 0) {

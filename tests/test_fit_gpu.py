@@ -82,6 +82,19 @@ def test_hub_row_larger_than_shared_memory(oracle_port):
     assert_same(a, b)
 
 
+def test_hub_edge_with_many_common_neighbours(oracle_port):
+    """Two hubs sharing 5000 neighbours and joined by an edge: that edge's
+    5001-term sum is a hub-edge item, streamed by a whole warp."""
+    k = 5000
+    leaves = np.arange(2, k + 2, dtype=np.int32)
+    U = np.concatenate([[0], np.zeros(k, np.int32), np.ones(k, np.int32)]).astype(np.int32)
+    V = np.concatenate([[1], leaves, leaves]).astype(np.int32)
+    W = graphs.uniform_weights(len(U), seed=4)
+    a = gpu_fit(k + 2, U, V, W)
+    b = oracle_port.fit(k + 2, U, V, W)
+    assert_same(a, b)
+
+
 def test_multigraph_and_self_loops(oracle_port):
     rng = np.random.default_rng(9)
     n = 30
