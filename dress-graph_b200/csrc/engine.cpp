@@ -49,6 +49,7 @@ Status Pinned::reserve(size_t bytes)
 }
 
 thread_local cudaMemPool_t tls_pool = nullptr;
+thread_local long long tls_launches = 0;
 
 Status Ctx::create(int dev, int sms, const dressx_config_t *config, int priority)
 {

@@ -128,7 +128,15 @@ void set_last_error(const Status &s);
 
 inline void count_h2d(size_t b) { engine().h2d_bytes += (long long)b; }
 inline void count_d2h(size_t b) { engine().d2h_bytes += (long long)b; }
-inline void count_launch(int n = 1) { engine().launches += n; }
+// Kernel launches are counted process-wide and per thread; a thread that
+// captures a CUDA graph measures the graph's launches on its own counter,
+// which launches of other threads in the meantime leave alone.
+extern thread_local long long tls_launches;
+inline void count_launch(int n = 1)
+{
+    engine().launches += n;
+    tls_launches += n;
+}
 
 // cudaMemcpyAsync that also counts the bytes it moves between host and device
 inline cudaError_t counted_memcpy(void *dst, const void *src, size_t n, cudaMemcpyKind kind, cudaStream_t st)

@@ -699,7 +699,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     long long pair_launches = 0;
     {
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-        const long long before = engine().launches.load();
+        const long long before = tls_launches;
         cudaGraph_t graph = nullptr;
         if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
             Status cs = enqueue_pair();
@@ -709,8 +709,9 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
             if (graph) cudaGraphDestroy(graph);
         }
         cudaGetLastError();                           // a failed capture leaves direct launches
-        pair_launches = engine().launches.load() - before;
+        pair_launches = tls_launches - before;
         engine().launches -= pair_launches;           // counted per replay below
+        tls_launches -= pair_launches;
     }
     struct GraphGuard {
         cudaGraphExec_t g;
