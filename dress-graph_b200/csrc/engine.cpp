@@ -9,6 +9,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <algorithm>
+
 #include "engine.h"
 
 namespace dress {
@@ -36,9 +38,19 @@ Pinned::~Pinned()
 Status Pinned::reserve(size_t bytes)
 {
     if (bytes <= cap_) return Status::Ok();
+    // Pinning host memory is slow and freeing it waits for the device, so
+    // the buffer grows at least twofold (and to at least 32 MiB): a stream
+    // of growing requests reallocates it a few times, not at every request.
+    const size_t want = std::max(bytes, std::max(2 * cap_, (size_t)32 << 20));
     if (base_) cudaFreeHost(base_);
     base_ = nullptr;
     cap_ = 0;
+    if (cudaMallocHost((void **)&base_, want) == cudaSuccess) {
+        cap_ = want;
+        return Status::Ok();
+    }
+    cudaGetLastError();
+    base_ = nullptr;
     if (cudaMallocHost((void **)&base_, bytes) != cudaSuccess) {
         cudaGetLastError();
         base_ = nullptr;

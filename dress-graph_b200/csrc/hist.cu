@@ -10,12 +10,14 @@
 // adjacent after the sort) and every NaN is a run of its own, as in the
 // reference's map.  A pass in which every segment has a single digit value
 // moves nothing and is skipped.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <thread>
+#include <condition_variable>
 #include <vector>
 
 #include "engine.h"
@@ -379,7 +381,8 @@ __global__ void k_seg_ends(long long R, const int *run_seg, long long *seg_end)
 }
 
 Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
-                       cudaStream_t st, int sms, std::vector<int64_t *> *pre, const std::vector<long long> *cap)
+                       cudaStream_t st, int sms, std::vector<int64_t *> *pre, const std::vector<long long> *cap,
+                       int max_threads)
 {
     const int nseg = res.nseg;
     outs.assign((size_t)nseg, nullptr);
@@ -415,35 +418,24 @@ Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vecto
         pageable.resize(2 * (size_t)R);
         host = pageable.data();
     }
-    // Large results: one part per host thread, balanced by bytes.  Each part
-    // is its own download; while the parts stream in, the threads allocate
-    // their segments' arrays and touch every page (the page faults of fresh
-    // memory cost more than the copy), then copy their part once it landed.
-    const int nthr = pinned && bytes > (64u << 20) && nseg > 1 ? host_threads(nseg) : 1;
-    std::vector<int> cut(1, 0);
-    {
-        const long long per = (2 * R + nthr - 1) / nthr;
-        long long acc = 0;
-        for (int sg = 0; sg < nseg; ++sg) {
-            acc += lens[(size_t)sg];
-            if (acc >= per * (long long)cut.size() && (int)cut.size() < nthr) cut.push_back(sg + 1);
-        }
-        if (cut.back() != nseg) cut.push_back(nseg);
-    }
-    const int parts = (int)cut.size() - 1;
+    // The output, runs [0, R) in segment order, is cut into one part per host
+    // thread, balanced by bytes; each part is its own download.  A thread
+    // allocates the arrays of the segments that start in its part, and after
+    // a barrier (a segment may reach into later parts) maps the pages of its
+    // part's share of the arrays while the downloads stream in -- the page
+    // faults of fresh memory cost more than the copy -- then copies its
+    // share once its part landed.  A final barrier precedes the trimming of
+    // given arrays to their length.
+    const int nthr = pinned && bytes > (64u << 20) ? std::min(max_threads, host_threads((long long)(bytes >> 23))) : 1;
+    const int parts = std::max(1, nthr);
+    std::vector<long long> pcut((size_t)parts + 1);
+    for (int t = 0; t <= parts; ++t) pcut[(size_t)t] = R * t / parts;
     std::vector<cudaEvent_t> ev((size_t)parts, nullptr);
     Status err;
     for (int t = 0; t < parts && err.ok(); ++t) {
-        // the part's runs: from the first run of its first segment to the
-        // end of its last non-empty segment
-        long long r0 = -1, r1 = -1;
-        for (int sg = cut[(size_t)t]; sg < cut[(size_t)t + 1]; ++sg)
-            if (lens[(size_t)sg] > 0) {
-                if (r0 < 0) r0 = first[(size_t)sg];
-                r1 = end[(size_t)sg];
-            }
-        if (r0 < 0) continue;
-        if (cudaEventCreateWithFlags(&ev[(size_t)t], cudaEventDisableTiming) != cudaSuccess) {
+        const long long r0 = pcut[(size_t)t], r1 = pcut[(size_t)t + 1];
+        if (r1 <= r0) continue;
+        if (cudaEventCreateWithFlags(&ev[(size_t)t], cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess) {
             ev[(size_t)t] = nullptr;
             err = Status::Err(DRESSX_ECUDA, "event creation failed");
             break;
@@ -453,75 +445,98 @@ Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vecto
         if (e == cudaSuccess) e = cudaEventRecord(ev[(size_t)t], st);
         if (e != cudaSuccess) err = Status::Err(DRESSX_ECUDA, std::string("histogram download: ") + cudaGetErrorString(e));
     }
-    // ready: parts whose download is complete (or -1 once the downloads failed)
+    // segments in part order: the first segment whose runs reach into each part
+    std::vector<int> seg0((size_t)parts + 1, nseg);
+    {
+        int sg = 0;
+        for (int t = 0; t < parts; ++t) {
+            while (sg < nseg && (lens[(size_t)sg] == 0 || first[(size_t)sg] + lens[(size_t)sg] / 2 <= pcut[(size_t)t]))
+                ++sg;
+            seg0[(size_t)t] = sg;
+        }
+    }
     std::vector<char> given((size_t)nseg, 0);    // segments that took a given array
-    std::atomic<int> ready{0};
     std::atomic<bool> nomem{false};
-    // A part's thread maps the pages of its arrays (a write to each page) while
-    // the part's download is in flight, and once it landed copies into the
-    // arrays mapped so far and then into fresh ones, whose page faults the
-    // copy takes itself.
+    std::mutex mu;
+    std::condition_variable cv;
+    int ready = 0;                               // parts landed; -1 once the downloads failed
+    int arrived[2] = {0, 0};                     // barrier counts
+    auto barrier = [&](int b) {
+        std::unique_lock<std::mutex> lk(mu);
+        if (++arrived[b] == parts) cv.notify_all();
+        else cv.wait(lk, [&] { return arrived[b] == parts; });
+    };
     auto part_work = [&](int t) {
-        const int s0 = cut[(size_t)t], s1 = cut[(size_t)t + 1];
-        // a segment's array: the one given for it when it fits (true), else a new one
-        auto alloc = [&](int sg) {
+        const long long p0 = pcut[(size_t)t], p1 = pcut[(size_t)t + 1];
+        // the segments starting in this part
+        for (int sg = seg0[(size_t)t]; sg < nseg && first[(size_t)sg] < p1; ++sg) {
             const size_t n = (size_t)lens[(size_t)sg] * sizeof(int64_t);
-            if (n && pre && (*pre)[(size_t)sg] && lens[(size_t)sg] <= (*cap)[(size_t)sg]) {
+            if (!n || first[(size_t)sg] < p0) continue;
+            if (pre && (*pre)[(size_t)sg] && lens[(size_t)sg] <= (*cap)[(size_t)sg]) {
                 outs[(size_t)sg] = (*pre)[(size_t)sg];
                 (*pre)[(size_t)sg] = nullptr;
                 given[(size_t)sg] = 1;
-                return true;
-            }
-            char *a = n ? (char *)std::malloc(n) : nullptr;
-            outs[(size_t)sg] = (int64_t *)a;
-            if (n && !a) nomem = true;
-            return false;
-        };
-        auto copy = [&](int sg) {
-            int64_t *a = outs[(size_t)sg];
-            if (!a) return;
-            const size_t n = (size_t)lens[(size_t)sg] * sizeof(int64_t);
-            std::memcpy(a, host + 2 * first[(size_t)sg], n);
-            if (given[(size_t)sg] && lens[(size_t)sg] < (*cap)[(size_t)sg]) {
-                // trim a given array (shrinking keeps the data)
-                void *r2 = std::realloc(a, n);
-                if (r2) outs[(size_t)sg] = (int64_t *)r2;
-            }
-        };
-        int sg = s0;
-        int r;
-        while ((r = ready.load()) >= 0 && r <= t) {
-            if (sg == s1) {
-                std::this_thread::yield();
                 continue;
             }
-            if (!alloc(sg)) {
-                char *a = (char *)outs[(size_t)sg];
-                const size_t n = (size_t)lens[(size_t)sg] * sizeof(int64_t);
-                if (a)
-                    for (size_t o = 0; o < n; o += 4096) ((volatile char *)a)[o] = 0;
+            outs[(size_t)sg] = (int64_t *)std::malloc(n);
+            if (!outs[(size_t)sg]) nomem = true;
+        }
+        barrier(0);
+        // this part's share of segment sg: runs [a, b)
+        auto share = [&](int sg, long long &a, long long &b) {
+            a = std::max(p0, first[(size_t)sg]);
+            b = std::min(p1, first[(size_t)sg] + lens[(size_t)sg] / 2);
+        };
+        if (parts > 1)
+            for (int sg = seg0[(size_t)t]; sg < nseg && first[(size_t)sg] < p1; ++sg) {
+                long long a, b;
+                share(sg, a, b);
+                char *o = (char *)outs[(size_t)sg];
+                if (b <= a || !o || given[(size_t)sg]) continue;
+                const size_t lo_b = (size_t)(a - first[(size_t)sg]) * 16, hi_b = (size_t)(b - first[(size_t)sg]) * 16;
+                for (size_t x = lo_b; x < hi_b; x += 4096) ((volatile char *)o)[x] = 0;
             }
-            ++sg;
+        bool ok;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return ready < 0 || ready > t; });
+            ok = ready > t;
         }
-        if (r < 0) return;
-        for (int q = s0; q < sg; ++q) copy(q);
-        for (int q = sg; q < s1; ++q) {
-            alloc(q);
-            copy(q);
-        }
+        if (ok)
+            for (int sg = seg0[(size_t)t]; sg < nseg && first[(size_t)sg] < p1; ++sg) {
+                long long a, b;
+                share(sg, a, b);
+                int64_t *o = outs[(size_t)sg];
+                if (b <= a || !o) continue;
+                std::memcpy(o + 2 * (a - first[(size_t)sg]), host + 2 * a, (size_t)(b - a) * 16);
+            }
+        barrier(1);
+        // trim the given arrays of the segments starting here (shrinking keeps the data)
+        for (int sg = seg0[(size_t)t]; sg < nseg && first[(size_t)sg] < p1; ++sg)
+            if (given[(size_t)sg] && first[(size_t)sg] >= p0 && lens[(size_t)sg] < (*cap)[(size_t)sg]) {
+                void *r2 = std::realloc(outs[(size_t)sg], (size_t)lens[(size_t)sg] * sizeof(int64_t));
+                if (r2) outs[(size_t)sg] = (int64_t *)r2;
+            }
     };
     std::vector<std::thread> th;
     if (parts > 1)
         for (int t = 0; t < parts; ++t) th.emplace_back(part_work, t);
     // this thread waits for the downloads in order and releases the parts
     for (int t = 0; t < parts && err.ok(); ++t) {
-        if (ev[(size_t)t] && cudaEventSynchronize(ev[(size_t)t]) != cudaSuccess)
+        if (ev[(size_t)t] && cudaEventSynchronize(ev[(size_t)t]) != cudaSuccess) {
             err = Status::Err(DRESSX_ECUDA, "histogram download failed");
-        else
+        } else {
+            std::lock_guard<std::mutex> lk(mu);
             ready = t + 1;
+            cv.notify_all();
+        }
     }
-    if (!err.ok()) ready = -1;
-    if (err.ok() && parts == 1) part_work(0);
+    if (!err.ok()) {
+        std::lock_guard<std::mutex> lk(mu);
+        ready = -1;
+        cv.notify_all();
+    }
+    if (parts == 1) part_work(0);
     for (auto &t : th) t.join();
     for (cudaEvent_t e : ev)
         if (e) cudaEventDestroy(e);

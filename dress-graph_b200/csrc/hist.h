@@ -24,10 +24,11 @@ Status histogram_download(HistResult &res, std::vector<std::vector<long long>> &
 // through the pinned staging buffer when one is given.  pre/cap (nullable):
 // malloc'd arrays that already exist per segment and their capacity in
 // int64 entries; a segment that fits takes its array (trimmed to length,
-// the entry cleared), the others get new ones.
+// the entry cleared), the others get new ones.  Large results are copied
+// out by up to max_threads host threads.
 Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
                        cudaStream_t st, int sms, std::vector<int64_t *> *pre = nullptr,
-                       const std::vector<long long> *cap = nullptr);
+                       const std::vector<long long> *cap = nullptr, int max_threads = 16);
 
 // Stable ascending sort of n unsigned 64-bit keys with a 32-bit payload
 // (LSD radix, 8-bit digits; digits equal on every key are skipped).  The

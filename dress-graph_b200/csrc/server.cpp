@@ -67,6 +67,9 @@ constexpr long long B200_SMEM_OPTIN = 232448;
 // buffer, and the sort / run-length scratch.
 constexpr long long HIST_BYTES_PER_VALUE = 56;
 
+// Pinned staging per lane and finisher at start-up (each grows on demand).
+constexpr size_t STAGE_START_BYTES = (size_t)64 << 20;
+
 // Largest whole-graph fit packed into batch launches.
 constexpr int PLAIN_BATCH_MAX_EDGES = 2048;
 
@@ -363,6 +366,9 @@ Status Server::start(const dressx_server_config_t *c)
         fins.push_back(c2);
         DRESS_TRY(c2->create(device, sms, &en.cfg, hi));
     }
+    // staging buffers pinned now rather than while requests are in flight
+    for (Lane *ln : lanes) ln->ctx.stage->reserve(STAGE_START_BYTES);
+    for (Ctx *c2 : fins) c2->stage->reserve(STAGE_START_BYTES);
     t0 = Clock::now();
     threads.emplace_back([this] { scheduler(); });
     for (Lane *ln : lanes) threads.emplace_back([this, ln] { lane_main(ln); });
@@ -768,19 +774,19 @@ Status collect_batch(Server *sv, Req *r, Ctx *ctx)
     p->edge_sweeps = (int64_t)st[ST_EDGE_ITERS];
     const long long n = (long long)st[ST_CURSOR];
     if (n <= 0) return Status::Ok();
+    // the histogram straight into its malloc'd array, through this
+    // finisher's pinned stage
     DevBuf<unsigned long long> alt;
     DRESS_TRY(alt.alloc((size_t)n, ctx->st));
-    std::vector<std::vector<long long>> out;
-    DRESS_TRY(histogram_segments(r->d_values.get(), alt.get(), std::vector<long long>{0},
-                                 std::vector<long long>{n}, out, ctx->st, sv->sms));
-    DRESS_CUDA_TRY(cudaStreamSynchronize(ctx->st));
-    const std::vector<long long> &flat = out[0];
-    if (!flat.empty()) {
-        p->hist_flat = (int64_t *)std::malloc(flat.size() * sizeof(int64_t));
-        if (!p->hist_flat) return Status::Err(DRESSX_ENOMEM, "host allocation of the histogram failed");
-        std::memcpy(p->hist_flat, flat.data(), flat.size() * sizeof(int64_t));
-        p->hist_len = (int)flat.size();
-    }
+    HistResult res;
+    DRESS_TRY(histogram_device(r->d_values.get(), alt.get(), std::vector<long long>{0}, std::vector<long long>{n}, res,
+                               ctx->st, sv->sms));
+    std::vector<int64_t *> outs;
+    std::vector<long long> lens;
+    // at most 8 copy threads: lanes and other finishers share the host
+    DRESS_TRY(histogram_fetch(res, outs, lens, ctx->stage, ctx->st, sv->sms, nullptr, nullptr, 8));
+    p->hist_flat = outs[0];
+    p->hist_len = (int)lens[0];
     return Status::Ok();
 }
 
