@@ -162,6 +162,10 @@ struct FitStats {
 };
 Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon,
                  int *iterations, double *delta, FitStats *stats, const Ctx &ctx);
+// The same fit in one launch for graphs whose state fits one SM (fit_small.cu);
+// `used` is false, and nothing is done, for the others.
+Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *iterations, double *delta,
+                 FitStats *stats, const Ctx &ctx, bool &used);
 
 // ---- Delta/Nabla requests (delta_nabla.cpp) ---------------------------------
 // edge_sweeps (nullable, n entries): live edges x sweeps summed over each

@@ -355,6 +355,12 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         return Status::Err(DRESSX_EINVAL, "graph has NULL edge arrays");
     const long long S = N > 0 ? g->adj_offset[N] : 0;
     if (N > 0 && (g->adj_offset[0] != 0 || S < 0)) return Status::Err(DRESSX_EINVAL, "bad adj_offset");
+    {
+        // small graphs: the whole fit in one launch
+        bool used = false;
+        DRESS_TRY(fit_small(g, max_iterations, epsilon, iterations, delta, stats, ctx, used));
+        if (used) return Status::Ok();
+    }
 
     cudaStream_t st = ctx.st;
     const int sms = ctx.num_sms;

@@ -1,0 +1,192 @@
+// fit_small.cu -- the single-graph fit of a small graph in one launch.
+//
+// Reference: libdress/src/dress.c:546-608 (the iteration driver) with the
+// vertex and edge phases of :556-591.  A graph whose whole fit state (edge
+// values twice, vertex norms) fits one SM's shared memory, with rows of at
+// most 31 neighbours, is fitted by one 512-thread CTA of the batch kernel as
+// a single whole-graph item: every sweep, the convergence test and the final
+// values in one launch, without per-sweep kernels or host round trips.  The
+// arithmetic is the batch kernel's, bit-identical to the reference's (sorted
+// Kahan-Babuska-Neumaier sums, separately rounded products).  The graph is
+// staged in shared memory as well.  Larger graphs, and graphs that carry
+// their own intercept tables, take the multi-kernel fit in fit_graph.cu.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <vector>
+
+#include "batch.h"
+#include "engine.h"
+
+namespace dress {
+
+namespace {
+constexpr int SMALL_GSIZE = 512;       // threads of the one group
+// Above about 3000 edges one SM takes longer than the multi-kernel fit over
+// the whole device (measured on G(n, m): 0.21-0.33 ms against 0.95 ms up to
+// 1500 edges, even at 3000, behind beyond).
+constexpr int SMALL_MAX_EDGES = 2048;
+constexpr int SMALL_MAX_DEG = 31;      // rows the register networks take (32 terms with the self term)
+
+// The checks of fit_graph's device validation, on the host: rows in order
+// and in range, edge ids and endpoints in range.
+bool small_graph_ok(p_dress_graph_t g, int &maxdeg)
+{
+    const int N = g->N, E = g->E;
+    maxdeg = 0;
+    for (int u = 0; u < N; ++u) {
+        const int b = g->adj_offset[u], e = g->adj_offset[u + 1];
+        if (e < b) return false;
+        maxdeg = std::max(maxdeg, e - b);
+        for (int s = b; s < e; ++s) {
+            const int x = g->adj_target[s], ei = g->adj_edge_idx[s];
+            if (x < 0 || x >= N || ei < 0 || ei >= E) return false;
+            if (s > b && x < g->adj_target[s - 1]) return false;
+        }
+    }
+    for (int e = 0; e < E; ++e)
+        if (g->U[e] < 0 || g->U[e] >= N || g->V[e] < 0 || g->V[e] >= N) return false;
+    return true;
+}
+}  // namespace
+
+Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *iterations, double *delta,
+                 FitStats *stats, const Ctx &ctx, bool &used)
+{
+    used = false;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int N = g->N, E = g->E;
+    if (E < 1 || E > SMALL_MAX_EDGES || N < 1 || (g->precompute_intercepts && g->intercept_offset))
+        return Status::Ok();
+    const long long S = g->adj_offset[N];
+    if (g->adj_offset[0] != 0 || S < 0) return Status::Ok();      // fit_graph reports it
+
+    // shape: one group of SMALL_GSIZE threads and the staged parent
+    int smem_optin = 0;
+    DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx.device));
+    const long long smem_cap = smem_optin - 1024;
+    // the state and the graph without its pairs must fit before the pairs are found
+    if (batch_group_bytes(E, N, 1, SMALL_GSIZE) + parent_layout(N, E, (int)S, 0, g->NW != nullptr, 1).bytes >
+        smem_cap)
+        return Status::Ok();
+    int maxdeg = 0;
+    if (!small_graph_ok(g, maxdeg)) return Status::Ok();       // fit_graph reports it
+    if (maxdeg > SMALL_MAX_DEG) return Status::Ok();
+
+    std::vector<int> ioff, pairs;
+    bool dup = false;                        // repeated neighbours: the merge walk pairs them as the reference does
+    merge_walk_pairs(g, ioff, pairs, maxdeg, dup);
+    const int T = (int)(pairs.size() / 2);
+    const int has_nw = g->NW != nullptr;
+    const ParentLayout PL = parent_layout(N, E, (int)S, T, has_nw, 1);
+
+    BatchLaunch L{};
+    L.gsize = SMALL_GSIZE;
+    L.groups = 1;
+    L.per_group = 0;
+    L.min_ctas = 1;
+    L.maxE = E;
+    L.maxN = N;
+    L.maxk = 1;
+    L.M = 2;                                 // smallest register network that holds a row
+    while (L.M < maxdeg + 1) L.M <<= 1;
+    L.parent_bytes = PL.bytes;
+    // The graph itself must be staged in shared memory too: read through L2
+    // by a single SM, the sweeps are latency-bound and the multi-kernel fit
+    // answers sooner (measured on G(2000, 10000): 3.9 ms against 1.3 ms).
+    L.stage = 1;
+    if ((long long)batch_smem_bytes(L) > smem_cap) return Status::Ok();
+
+    // the packed parent: arrays of the graph, the pairs, the current values
+    std::vector<unsigned char> packed((size_t)PL.bytes, 0);
+    unsigned char *b = packed.data();
+    std::memcpy(b + PL.U, g->U, (size_t)E * 4);
+    std::memcpy(b + PL.V, g->V, (size_t)E * 4);
+    std::memcpy(b + PL.w, g->edge_weight, (size_t)E * 8);
+    std::memcpy(b + PL.row_off, g->adj_offset, (size_t)(N + 1) * 4);
+    if (S) std::memcpy(b + PL.row_eid, g->adj_edge_idx, (size_t)S * 4);
+    std::memcpy(b + PL.ioff, ioff.data(), (size_t)(E + 1) * 4);
+    if (T) std::memcpy(b + PL.pairs, pairs.data(), (size_t)T * 8);
+    if (has_nw) std::memcpy(b + PL.nw, g->NW, (size_t)N * 8);
+    std::memcpy(b + PL.dinit, g->edge_dress, (size_t)E * 8);
+
+    cudaStream_t st = ctx.st;
+    DevBuf<unsigned char> d_data;
+    DevBuf<double> d_values;
+    DevBuf<unsigned long long> d_stats;
+    DevBuf<ParentDesc> d_desc;
+    DevBuf<Chunk> d_chunk;
+    DevBuf<int> d_counter;
+    DRESS_TRY(d_data.alloc(packed.size(), st));
+    DRESS_TRY(d_values.alloc((size_t)E + N, st));
+    DRESS_TRY(d_stats.alloc(ST_WORDS, st));
+    DRESS_TRY(d_desc.alloc(1, st));
+    DRESS_TRY(d_chunk.alloc(1, st));
+    DRESS_TRY(d_counter.alloc(1, st));
+    ParentDesc P{};
+    P.N = N;
+    P.E = E;
+    P.S = (int)S;
+    P.T = T;
+    P.kind = ITEM_PLAIN;
+    P.k = 0;
+    P.fwd = g->variant == DRESS_VARIANT_FORWARD || g->variant == DRESS_VARIANT_BACKWARD;
+    P.max_iter = max_iterations;
+    P.eps = epsilon;
+    P.has_nw = has_nw;
+    P.has_dinit = 1;
+    P.data = d_data.get();
+    P.values = d_values.get();
+    P.stats = d_stats.get();
+    P.offset = 0;
+    P.stride = 1;
+    const Chunk ch{0, 1, 0};
+    DRESS_CUDA_TRY(counted_memcpy(d_data.get(), packed.data(), packed.size(), cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(counted_memcpy(d_desc.get(), &P, sizeof P, cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(counted_memcpy(d_chunk.get(), &ch, sizeof ch, cudaMemcpyHostToDevice, st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_stats.get(), 0, ST_WORDS * sizeof(unsigned long long), st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_counter.get(), 0, sizeof(int), st));
+    L.parents = d_desc.get();
+    L.chunks = d_chunk.get();
+    L.nchunks = 1;
+    L.chunk_counter = d_counter.get();
+
+    cudaEvent_t e0, e1;
+    DRESS_CUDA_TRY(cudaEventCreate(&e0));
+    DRESS_CUDA_TRY(cudaEventCreate(&e1));
+    struct EvGuard {
+        cudaEvent_t a, b;
+        ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } guard{e0, e1};
+    const double setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    DRESS_CUDA_TRY(cudaEventRecord(e0, st));
+    DRESS_TRY(launch_batch(L, ctx.num_sms, st));
+    DRESS_CUDA_TRY(cudaEventRecord(e1, st));
+
+    unsigned long long sv[ST_WORDS];
+    DRESS_CUDA_TRY(counted_memcpy(sv, d_stats.get(), sizeof sv, cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(counted_memcpy(g->edge_dress, d_values.get(), (size_t)E * sizeof(double),
+                                   cudaMemcpyDeviceToHost, st));
+    DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    // the norms of the last sweep (none without sweeps), as fit_graph leaves them
+    if (sv[ST_SWEEPS] > 0) {
+        DRESS_CUDA_TRY(counted_memcpy(g->vertex_dress, d_values.get() + E, (size_t)N * sizeof(double),
+                                       cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    float it_ms = 0.f;
+    cudaEventElapsedTime(&it_ms, e0, e1);
+    if (iterations) *iterations = (int)(long long)sv[ST_ITERATIONS];
+    if (delta && sv[ST_SWEEPS] > 0) std::memcpy(delta, &sv[ST_DELTA], sizeof(double));
+    if (stats) {
+        *stats = FitStats{};
+        stats->T = T;
+        stats->sweeps = (int)sv[ST_SWEEPS];
+        stats->setup_ms = setup_ms;
+        stats->iterate_ms = it_ms;
+    }
+    used = true;
+    return Status::Ok();
+}
+
+}  // namespace dress
