@@ -17,8 +17,12 @@
 //   * each group iterates its subgraph to its own convergence (state d, d_next,
 //     vertex norms in shared memory) and appends the live edges' values to the
 //     request's value segment (the histogram is built afterwards, hist.cu).
+#include <cooperative_groups.h>
+
 #include "batch.h"
 #include "common.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace dress {
 namespace {
@@ -182,9 +186,64 @@ __device__ __forceinline__ int group_sum(const Group &g, int v, double *red, int
     return (int)s;
 }
 
-template <int M>
+// ---- a whole graph over a thread-block cluster ---------------------------------
+// Every thread of the cluster is one member of the group; the state arrays are
+// distributed over the CTAs' shared memory, each CTA holding the elements its
+// own threads update in the group loops (element i, visited by group thread
+// i mod size, lives in CTA (i / B) mod n at ((i / (B n)) B + i mod B), B the
+// CTA's threads, n the CTAs).  Other elements are read through distributed
+// shared memory.  sync() is the cluster barrier, which also orders the
+// shared-memory writes of every CTA (no thread spins).
+struct ClusterGroup {
+    int t, size;
+    double *wsl;                 // this CTA's per-warp reduction slots, two parities
+    double *const *part;         // every CTA's two partial slots
+    int ncta;
+    __device__ __forceinline__ void sync() const { cg::this_cluster().sync(); }
+};
+
+struct DArr {
+    double *const *tab;          // every CTA's slice (generic addresses)
+    int lb, lnc;                 // log2 of the CTA's threads and of the CTAs
+    __device__ __forceinline__ double &operator[](int i) const
+    {
+        const int r = (i >> lb) & ((1 << lnc) - 1);
+        const int l = ((i >> (lb + lnc)) << lb) | (i & ((1 << lb) - 1));
+        return tab[r][l];
+    }
+};
+
+template <class Op>
+__device__ __forceinline__ double cluster_reduce(const ClusterGroup &g, double v, int parity, Op op)
+{
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int nw = (int)blockDim.x >> 5;
+    if ((threadIdx.x & 31) == 0) g.wsl[parity * nw + (threadIdx.x >> 5)] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = g.wsl[parity * nw];
+        for (int i = 1; i < nw; ++i) m = op(m, g.wsl[parity * nw + i]);
+        g.part[cg::this_cluster().block_rank()][parity] = m;
+    }
+    g.sync();
+    double m = g.part[0][parity];
+    for (int r = 1; r < g.ncta; ++r) m = op(m, g.part[r][parity]);
+    return m;
+}
+
+__device__ __forceinline__ double group_max(const ClusterGroup &g, double v, double *, int parity)
+{
+    return fmax(0.0, cluster_reduce(g, v, parity, [](double a, double b) { return fmax(a, b); }));
+}
+
+__device__ __forceinline__ int group_sum(const ClusterGroup &g, int v, double *, int parity)
+{
+    return (int)cluster_reduce(g, (double)v, parity, [](double a, double b) { return a + b; });
+}
+
+template <int M, class Grp, class Arr>
 __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
-                         const Group &g, double *d0, double *d1, double *vd, double *red, int *ks,
+                         const Grp &g, Arr d0, Arr d1, Arr vd, double *red, int *ks,
                          unsigned long long *slot)
 {
     const int N = P.N, E = P.E;
@@ -270,7 +329,7 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
         }
         const double m = group_max(g, lmax, red, (it & 1));
         last = m;
-        double *t = d0;
+        const Arr t = d0;
         d0 = d1;
         d1 = t;
         g.sync();
@@ -432,7 +491,97 @@ Status launch_m(const BatchLaunch &L, int sms, cudaStream_t st)
     return launch_mg<M, false, 1>(L, sms, st);
 }
 
+// One whole-graph fit (ParentDesc of kind ITEM_PLAIN) by one cluster of
+// CL_THREADS-thread CTAs.  Shared memory of a CTA: its slices of d, d_next
+// and the vertex norms (per_e, per_e and per_n doubles), the warp slots, its
+// two partials, and the tables of every CTA's slices.
+constexpr int CL_THREADS = 512, CL_LB = 9;
+constexpr int CL_MAX_CTAS = 16;
+
+template <int M>
+__global__ void __launch_bounds__(CL_THREADS, 1) k_fit_cluster(const ParentDesc *pp, int per_e, int per_n, int lnc)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int nc = (int)cl.num_blocks();
+    double *s_d0 = (double *)smem;
+    double *s_d1 = s_d0 + per_e;
+    double *s_vd = s_d1 + per_e;
+    double *wsl = s_vd + per_n;
+    double *part = wsl + 2 * (CL_THREADS / 32);
+    double **tab = (double **)(part + 2);          // [4][CL_MAX_CTAS]: d0, d1, vd, partials
+    if ((int)threadIdx.x < nc) {
+        const unsigned r = threadIdx.x;
+        tab[0 * CL_MAX_CTAS + r] = cl.map_shared_rank(s_d0, r);
+        tab[1 * CL_MAX_CTAS + r] = cl.map_shared_rank(s_d1, r);
+        tab[2 * CL_MAX_CTAS + r] = cl.map_shared_rank(s_vd, r);
+        tab[3 * CL_MAX_CTAS + r] = cl.map_shared_rank(part, r);
+    }
+    cl.sync();                                      // tables ready, every CTA running
+    const ParentDesc P = *pp;
+    const ParentLayout PL = parent_layout(P.N, P.E, P.S, P.T, P.has_nw, P.has_dinit);
+    const View G = view_of(P.data, PL, P);
+    const ClusterGroup g{(int)cl.block_rank() * CL_THREADS + (int)threadIdx.x, nc * CL_THREADS, wsl,
+                         (double *const *)(tab + 3 * CL_MAX_CTAS), nc};
+    const DArr d0{tab + 0 * CL_MAX_CTAS, CL_LB, lnc}, d1{tab + 1 * CL_MAX_CTAS, CL_LB, lnc},
+        vd{tab + 2 * CL_MAX_CTAS, CL_LB, lnc};
+    fit_item<M>(P, G, 0, g, d0, d1, vd, nullptr, nullptr, nullptr);
+    cl.sync();                                      // no CTA leaves while others read its memory
+}
+
+template <int M>
+Status launch_cluster_m(const ParentDesc *d_parent, int E, int N, int lnc, int sms, cudaStream_t st)
+{
+    const int nc = 1 << lnc, span = nc * CL_THREADS;
+    const int per_e = ((E + span - 1) / span) * CL_THREADS, per_n = ((N + span - 1) / span) * CL_THREADS;
+    const size_t smem = (size_t)(2 * per_e + per_n + 2 * (CL_THREADS / 32) + 2) * sizeof(double) +
+                        4 * CL_MAX_CTAS * sizeof(double *);
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (nc > 8) DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster<M>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)nc);
+    cfg.blockDim = dim3(CL_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)nc;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_fit_cluster<M>, &cfg) != cudaSuccess || clusters < 1) {
+        cudaGetLastError();
+        return Status::Err(DRESSX_EUNSUPPORTED, "cluster fit does not fit the device");
+    }
+    count_launch();
+    DRESS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_fit_cluster<M>, d_parent, per_e, per_n, lnc));
+    (void)sms;
+    return Status::Ok();
+}
+
 }  // namespace
+
+size_t cluster_fit_smem_bytes(int E, int N, int lnc)
+{
+    const int span = (1 << lnc) * CL_THREADS;
+    const int per_e = ((E + span - 1) / span) * CL_THREADS, per_n = ((N + span - 1) / span) * CL_THREADS;
+    return (size_t)(2 * per_e + per_n + 2 * (CL_THREADS / 32) + 2) * sizeof(double) + 4 * CL_MAX_CTAS * sizeof(double *);
+}
+
+Status launch_cluster_fit(const ParentDesc *d_parent, int E, int N, int M, int lnc, int sms, cudaStream_t st)
+{
+    if (lnc < 0 || (1 << lnc) > CL_MAX_CTAS) return Status::Err(DRESSX_EINVAL, "cluster size out of range");
+    switch (M) {
+    case 2: return launch_cluster_m<2>(d_parent, E, N, lnc, sms, st);
+    case 4: return launch_cluster_m<4>(d_parent, E, N, lnc, sms, st);
+    case 8: return launch_cluster_m<8>(d_parent, E, N, lnc, sms, st);
+    case 16: return launch_cluster_m<16>(d_parent, E, N, lnc, sms, st);
+    case 32: return launch_cluster_m<32>(d_parent, E, N, lnc, sms, st);
+    default: return Status::Err(DRESSX_EUNSUPPORTED, "cluster fit network size out of range");
+    }
+}
 
 long long batch_group_bytes(int maxE, int maxN, int maxk, int gsize)
 {

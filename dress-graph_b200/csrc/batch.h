@@ -80,6 +80,12 @@ struct BatchLaunch {
 };
 
 Status launch_batch(const BatchLaunch &L, int sms, cudaStream_t st);
+// One whole-graph fit (the ITEM_PLAIN descriptor at d_parent) by one cluster
+// of 2^lnc CTAs whose shared memory holds the state (cluster_fit_smem_bytes
+// per CTA); M is the register network size.  DRESSX_EUNSUPPORTED when such a
+// cluster cannot be placed.
+Status launch_cluster_fit(const ParentDesc *d_parent, int E, int N, int M, int lnc, int sms, cudaStream_t st);
+size_t cluster_fit_smem_bytes(int E, int N, int lnc);
 size_t batch_smem_bytes(const BatchLaunch &L);
 // Shared memory of one group's state (edge values twice, vertex norms,
 // reduction slots, the k mask vertices); a graph is batchable only when one

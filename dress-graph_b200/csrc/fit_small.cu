@@ -1,4 +1,4 @@
-// fit_small.cu -- the single-graph fit of a small graph in one launch.
+// fit_small.cu -- the single-graph fit of a small or mid-size graph in one launch.
 //
 // Reference: libdress/src/dress.c:546-608 (the iteration driver) with the
 // vertex and edge phases of :556-591.  A graph whose whole fit state (edge
@@ -8,8 +8,11 @@
 // values in one launch, without per-sweep kernels or host round trips.  The
 // arithmetic is the batch kernel's, bit-identical to the reference's (sorted
 // Kahan-Babuska-Neumaier sums, separately rounded products).  The graph is
-// staged in shared memory as well.  Larger graphs, and graphs that carry
-// their own intercept tables, take the multi-kernel fit in fit_graph.cu.
+// staged in shared memory as well.  Graphs of up to CLUSTER_MAX_EDGES edges
+// that do not fit one CTA run on a thread-block cluster instead, the state
+// spread over its CTAs' distributed shared memory (batch.cu,
+// k_fit_cluster).  Larger graphs, and graphs that carry their own intercept
+// tables, take the multi-kernel fit in fit_graph.cu.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -26,6 +29,13 @@ constexpr int SMALL_GSIZE = 512;       // threads of the one group
 // the whole device (measured on G(n, m): 0.21-0.33 ms against 0.95 ms up to
 // 1500 edges, even at 3000, behind beyond).
 constexpr int SMALL_MAX_EDGES = 2048;
+// Beyond that, up to this many edges, one cluster of 8 CTAs holds the state
+// in its distributed shared memory and runs the fit in one launch.  Measured
+// on G(n, m) against the multi-kernel fit: 0.64 / 1.23 ms at 3000 edges,
+// 1.11 / 1.26 ms at 8000, 1.57 / 1.44 ms at 10000, 8.4 / 1.8 ms at 60000
+// (the per-thread load chains of eight SMs are latency-bound; clusters of 16
+// CTAs measured no better).
+constexpr int CLUSTER_MAX_EDGES = 8192;
 constexpr int SMALL_MAX_DEG = 31;      // rows the register networks take (32 terms with the self term)
 
 // The checks of fit_graph's device validation, on the host: rows in order
@@ -56,19 +66,26 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     used = false;
     const auto t0 = std::chrono::steady_clock::now();
     const int N = g->N, E = g->E;
-    if (E < 1 || E > SMALL_MAX_EDGES || N < 1 || (g->precompute_intercepts && g->intercept_offset))
+    if (E < 1 || E > CLUSTER_MAX_EDGES || N < 1 || (g->precompute_intercepts && g->intercept_offset))
         return Status::Ok();
     const long long S = g->adj_offset[N];
     if (g->adj_offset[0] != 0 || S < 0) return Status::Ok();      // fit_graph reports it
 
-    // shape: one group of SMALL_GSIZE threads and the staged parent
+    // shape: one group of SMALL_GSIZE threads and the staged parent (the state
+    // and the graph without its pairs must fit before the pairs are found),
+    // else a cluster of 8 CTAs (16 when 8 cannot hold the state)
     int smem_optin = 0;
     DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx.device));
     const long long smem_cap = smem_optin - 1024;
-    // the state and the graph without its pairs must fit before the pairs are found
-    if (batch_group_bytes(E, N, 1, SMALL_GSIZE) + parent_layout(N, E, (int)S, 0, g->NW != nullptr, 1).bytes >
-        smem_cap)
-        return Status::Ok();
+    bool one_cta = E <= SMALL_MAX_EDGES &&
+                   batch_group_bytes(E, N, 1, SMALL_GSIZE) +
+                           parent_layout(N, E, (int)S, 0, g->NW != nullptr, 1).bytes <= smem_cap;
+    int lnc = -1;
+    if (!one_cta) {
+        if ((long long)cluster_fit_smem_bytes(E, N, 3) <= smem_cap) lnc = 3;
+        else if ((long long)cluster_fit_smem_bytes(E, N, 4) <= smem_cap) lnc = 4;
+        else return Status::Ok();
+    }
     int maxdeg = 0;
     if (!small_graph_ok(g, maxdeg)) return Status::Ok();       // fit_graph reports it
     if (maxdeg > SMALL_MAX_DEG) return Status::Ok();
@@ -91,11 +108,17 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     L.M = 2;                                 // smallest register network that holds a row
     while (L.M < maxdeg + 1) L.M <<= 1;
     L.parent_bytes = PL.bytes;
-    // The graph itself must be staged in shared memory too: read through L2
-    // by a single SM, the sweeps are latency-bound and the multi-kernel fit
-    // answers sooner (measured on G(2000, 10000): 3.9 ms against 1.3 ms).
+    // On one CTA the graph itself must be staged in shared memory too: read
+    // through L2 by a single SM, the sweeps are latency-bound and the
+    // multi-kernel fit answers sooner (measured on G(2000, 10000): 3.9 ms
+    // against 1.3 ms).
     L.stage = 1;
-    if ((long long)batch_smem_bytes(L) > smem_cap) return Status::Ok();
+    if (one_cta && (long long)batch_smem_bytes(L) > smem_cap) {
+        one_cta = false;
+        if ((long long)cluster_fit_smem_bytes(E, N, 3) <= smem_cap) lnc = 3;
+        else if ((long long)cluster_fit_smem_bytes(E, N, 4) <= smem_cap) lnc = 4;
+        else return Status::Ok();
+    }
 
     // the packed parent: arrays of the graph, the pairs, the current values
     std::vector<unsigned char> packed((size_t)PL.bytes, 0);
@@ -160,7 +183,13 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     } guard{e0, e1};
     const double setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     DRESS_CUDA_TRY(cudaEventRecord(e0, st));
-    DRESS_TRY(launch_batch(L, ctx.num_sms, st));
+    if (one_cta) {
+        DRESS_TRY(launch_batch(L, ctx.num_sms, st));
+    } else {
+        Status ls = launch_cluster_fit(d_desc.get(), E, N, L.M, lnc, ctx.num_sms, st);
+        if (ls.code == DRESSX_EUNSUPPORTED) return Status::Ok();     // the multi-kernel fit takes it
+        DRESS_TRY(ls);
+    }
     DRESS_CUDA_TRY(cudaEventRecord(e1, st));
 
     unsigned long long sv[ST_WORDS];

@@ -60,6 +60,20 @@ def test_er2000_all_variants(oracle_port, variant, weighted):
     assert_same(a, b)
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("n,m", [(300, 1200), (1500, 6000)])
+def test_one_launch_fits(oracle_port, variant, n, m):
+    """Graphs fitted in one launch: up to 2048 edges by one CTA with the
+    graph in shared memory, up to 8192 by a cluster of CTAs whose
+    distributed shared memory holds the state."""
+    n, U, V = graphs.erdos_renyi(n, m, seed=9)
+    W = graphs.uniform_weights(m, seed=5)
+    NW = np.random.default_rng(2).uniform(0.5, 2.0, n)
+    a = gpu_fit(n, U, V, W, NW, variant=variant)
+    b = oracle_port.fit(n, U, V, W, NW, variant=variant)
+    assert_same(a, b)
+
+
 @pytest.mark.parametrize("pre", [0, 1])
 def test_powerlaw_bins(oracle_port, pre):
     """Chung-Lu graph whose rows and triangle counts fill every bin
