@@ -71,9 +71,11 @@ Status Ctx::create(int dev, int sms, const dressx_config_t *config, int priority
     DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, priority));
     DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, priority));
     DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&side2, cudaStreamNonBlocking, priority));
+    DRESS_CUDA_TRY(cudaStreamCreateWithPriority(&side3, cudaStreamNonBlocking, priority));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join2, cudaEventDisableTiming));
+    DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join3, cudaEventDisableTiming));
     stage = new Pinned();
     return Status::Ok();
 }
@@ -83,14 +85,17 @@ void Ctx::destroy()
     if (st) cudaStreamSynchronize(st);
     if (side) cudaStreamSynchronize(side);
     if (side2) cudaStreamSynchronize(side2);
+    if (side3) cudaStreamSynchronize(side3);
     if (fork) cudaEventDestroy(fork);
     if (join) cudaEventDestroy(join);
     if (join2) cudaEventDestroy(join2);
+    if (join3) cudaEventDestroy(join3);
     if (st) cudaStreamDestroy(st);
     if (side) cudaStreamDestroy(side);
     if (side2) cudaStreamDestroy(side2);
-    st = side = side2 = nullptr;
-    fork = join = join2 = nullptr;
+    if (side3) cudaStreamDestroy(side3);
+    st = side = side2 = side3 = nullptr;
+    fork = join = join2 = join3 = nullptr;
     delete stage;
     stage = nullptr;
 }

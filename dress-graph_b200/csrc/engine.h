@@ -102,7 +102,8 @@ struct Ctx {
     cudaStream_t st = nullptr;             // main stream
     cudaStream_t side = nullptr;           // concurrent hub work of the single-graph fit
     cudaStream_t side2 = nullptr;          // ... and its block items below the hubs
-    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
+    cudaStream_t side3 = nullptr;          // ... and its thread-per-item bins
+    cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr, join3 = nullptr;
     const dressx_config_t *cfg = nullptr;
     Pinned *stage = nullptr;               // host staging of this context's uploads and downloads
     // priority: CUDA stream priority of both streams (0 = default; lower

@@ -674,7 +674,8 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         s.skey = d_skey.get(); s.sbase = lim[0];
         s.tkey = d_tkey.get(); s.tbase = lim[2];
     }
-    LaunchCfg lc{sms, block_cap, vblock_cap, st, ctx.side, ctx.side2, ctx.fork, ctx.join, ctx.join2};
+    LaunchCfg lc{sms, block_cap, vblock_cap, st, ctx.side, ctx.side2, ctx.fork, ctx.join, ctx.join2,
+                 E <= BRANCH_MAX_EDGES ? ctx.side3 : nullptr, ctx.join3};
     double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + E};
     double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + E};
 
