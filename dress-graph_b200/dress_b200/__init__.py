@@ -129,6 +129,7 @@ class Graph:
                     _libc.free(ctypes.cast(p, ctypes.c_void_p))
         if not self.ptr:
             raise ValueError("dress_init_graph rejected the graph (vertex id out of range?)")
+        self.addr = ctypes.cast(self.ptr, ctypes.c_void_p).value     # for packed request arrays
         self.N = int(n_vertices)
         self.E = int(U.size)
 
@@ -281,7 +282,7 @@ def hist_requests(graphs, kind, k, max_iterations=100, epsilon=1e-6, n_samples=0
     n = len(graphs)
     reqs = (_abi.HistRequest * n)()
     v = _request_view(reqs)
-    v["graph"] = [ctypes.cast(g.ptr, ctypes.c_void_p).value for g in graphs]
+    v["graph"] = [g.addr for g in graphs]
     v["kind"] = int(kind)
     v["k"] = int(k)
     v["max_iterations"] = int(max_iterations)
