@@ -34,8 +34,11 @@ __device__ __forceinline__ void cmx(double &a, double &b)
     b = hi;
 }
 
-// Bitonic network (single-direction form) on the first m registers.
-template <int m, int M>
+// Bitonic network (single-direction form) on the first m registers, without
+// the comparators whose upper slot is S or beyond: slots from S on hold
+// +inf, and every comparator keeps the larger value in its upper slot, so
+// those slots never change and their comparators do nothing.
+template <int m, int S, int M>
 __device__ __forceinline__ void net(double (&a)[M])
 {
 #pragma unroll
@@ -43,14 +46,14 @@ __device__ __forceinline__ void net(double (&a)[M])
 #pragma unroll
         for (int i = 0; i < m; ++i) {
             int j = i ^ (k - 1);
-            if (j > i) cmx(a[i], a[j]);
+            if (j > i && j < S) cmx(a[i], a[j]);
         }
 #pragma unroll
         for (int s = k >> 2; s > 0; s >>= 1) {
 #pragma unroll
             for (int i = 0; i < m; ++i) {
                 int j = i ^ s;
-                if (j > i) cmx(a[i], a[j]);
+                if (j > i && j < S) cmx(a[i], a[j]);
             }
         }
     }
@@ -58,8 +61,9 @@ __device__ __forceinline__ void net(double (&a)[M])
 
 // Sorted KBN of the self term and the live ones among cnt stored terms
 // (term(j, t) yields stored term j and whether it is alive) in a register
-// network of Mi > cnt slots; dead and unused slots hold +inf.
-template <int Mi, class Term>
+// network of Mi > cnt slots, of which the first S are used (S = cnt + 1
+// when known at compile time, else Mi); dead and unused slots hold +inf.
+template <int Mi, int S, class Term>
 __device__ __forceinline__ double net_sum(double self, int cnt, Term term)
 {
     double a[Mi];
@@ -68,7 +72,7 @@ __device__ __forceinline__ double net_sum(double self, int cnt, Term term)
 #pragma unroll
     for (int j = 1; j < Mi; ++j) {
         a[j] = DRESS_INF;
-        if (j <= cnt) {
+        if (j < S && j <= cnt) {
             double t;
             if (term(j - 1, t)) {
                 a[j] = t;
@@ -76,12 +80,29 @@ __device__ __forceinline__ double net_sum(double self, int cnt, Term term)
             }
         }
     }
-    net<Mi, Mi>(a);
+    net<Mi, S, Mi>(a);
     double s = a[0], c = 0.0;
 #pragma unroll
     for (int i = 1; i < Mi; ++i)
         if (i < n) kbn_step(s, c, a[i]);
     return dadd(s, c);
+}
+
+// Networks of 2, 4, 6, 8, 12 and 16 slots (the comparators of the unused
+// tail dropped), the full M-slot network beyond.  A few sizes only: the
+// warps of an SM fit subgraphs of different degrees at once, and one
+// network per degree measured slower on such batches (instruction cache).
+template <int M, class Term>
+__device__ __forceinline__ double sum_pruned(double self, int cnt, Term term)
+{
+    const int S = cnt + 1;
+    if (S <= 2) return net_sum<2, 2>(self, cnt, term);
+    if (M >= 4 && S <= 4) return net_sum<(M >= 4 ? 4 : 2), (M >= 4 ? 4 : 2)>(self, cnt, term);
+    if (M >= 8 && S <= 6) return net_sum<(M >= 8 ? 8 : 2), (M >= 8 ? 6 : 2)>(self, cnt, term);
+    if (M >= 8 && S <= 8) return net_sum<(M >= 8 ? 8 : 2), (M >= 8 ? 8 : 2)>(self, cnt, term);
+    if (M >= 16 && S <= 12) return net_sum<(M >= 16 ? 16 : 2), (M >= 16 ? 12 : 2)>(self, cnt, term);
+    if (M >= 16 && S <= 16) return net_sum<(M >= 16 ? 16 : 2), (M >= 16 ? 16 : 2)>(self, cnt, term);
+    return net_sum<M, M>(self, cnt, term);
 }
 
 // The smallest network that holds the item: most items of sparse subgraphs
@@ -90,11 +111,7 @@ template <int M, class Term>
 __device__ __forceinline__ double item_sum(double self, int cnt, Term term)
 {
     if (cnt == 0) return dadd(self, 0.0);
-    if (cnt < 2) return net_sum<2>(self, cnt, term);
-    if (M >= 4 && cnt < 4) return net_sum<(M >= 4 ? 4 : 2)>(self, cnt, term);
-    if (M >= 8 && cnt < 8) return net_sum<(M >= 8 ? 8 : 2)>(self, cnt, term);
-    if (M >= 16 && cnt < 16) return net_sum<(M >= 16 ? 16 : 2)>(self, cnt, term);
-    return net_sum<M>(self, cnt, term);
+    return sum_pruned<M>(self, cnt, term);
 }
 
 __device__ __forceinline__ long long binom_d(int n, int k)
