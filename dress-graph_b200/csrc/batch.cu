@@ -262,10 +262,13 @@ __device__ __forceinline__ int group_sum(const ClusterGroup &g, int v, double *,
     return (int)cluster_reduce(g, (double)v, parity, [](double a, double b) { return a + b; });
 }
 
+// eb (nullable): E bits of group memory, set for the live edges of a Delta
+// subgraph; with them a term's liveness is one bit instead of its endpoints'
+// lookup against the deleted vertices.
 template <int M, class Grp, class Arr>
 __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
                          const Grp &g, Arr d0, Arr d1, Arr vd, double *red, int *ks,
-                         unsigned long long *slot)
+                         unsigned long long *slot, unsigned *eb)
 {
     const int N = P.N, E = P.E;
     const long long s = P.ranks ? P.ranks[item] : P.offset + item * P.stride;
@@ -302,12 +305,23 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
     Mask mk{P.kind, P.kind == ITEM_PLAIN ? 0 : P.k, ks};
 
     // ---- live edges, initial values -----------------------------------------
+    // a warp's lanes take 32 consecutive edges, so a ballot is a word of bits
+    const bool bits = eb && P.kind == ITEM_DELTA;
     int live = 0;
-    for (int e = g.t; e < E; e += g.size) {
-        live += mk.alive(G.U[e]) && mk.alive(G.V[e]);
-        d0[e] = P.has_dinit ? G.dinit[e] : 1.0;
+    for (int b0 = g.t & ~31; b0 < E; b0 += g.size) {
+        const int e = b0 + (g.t & 31);
+        const bool al = e < E && mk.alive(G.U[e]) && mk.alive(G.V[e]);
+        if (e < E) d0[e] = P.has_dinit ? G.dinit[e] : 1.0;
+        const unsigned word = __ballot_sync(0xffffffffu, al);
+        if (bits && (g.t & 31) == 0) eb[b0 >> 5] = word;
+        live += al;
     }
+    g.sync();                                    // the bits and initial values, group-wide
     live = group_sum(g, live, red, 0);
+    // is edge e live (given one of its endpoints is)
+    auto edge_live = [&](int e, int other) {
+        return bits ? ((eb[e >> 5] >> (e & 31)) & 1u) != 0 : mk.alive(other);
+    };
     if (live == 0 && P.kind != ITEM_PLAIN) {   // the reference skips edgeless subgraphs
         g.sync();
         return;
@@ -322,7 +336,7 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
             const int rb = G.row_off[u], deg = G.row_off[u + 1] - rb;
             vd[u] = dsqrt(item_sum<M>(dmul(4.0, mk.weight(u, G.nw)), deg, [&](int j, double &t) {
                 const int e = G.row_eid[rb + j];
-                if (!mk.alive(G.U[e] + G.V[e] - u)) return false;
+                if (P.kind == ITEM_DELTA && !edge_live(e, G.U[e] + G.V[e] - u)) return false;
                 t = dmul(G.w[e], d0[e]);
                 return true;
             }));
@@ -331,14 +345,15 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
         double lmax = 0.0;
         for (int e = g.t; e < E; e += g.size) {
             const int u = G.U[e], v = G.V[e];
-            if (!(mk.alive(u) && mk.alive(v))) continue;
+            if (P.kind == ITEM_DELTA && !(bits ? ((eb[e >> 5] >> (e & 31)) & 1u) != 0 : mk.alive(u) && mk.alive(v)))
+                continue;
             const double own = dmul(G.w[e], d0[e]);
             const double a4u = dmul(4.0, mk.weight(u, G.nw));
             const double self = P.fwd ? dadd(a4u, own) : dadd(dadd(a4u, dmul(4.0, mk.weight(v, G.nw))), dmul(2.0, own));
             const int pb = G.ioff[e], np = G.ioff[e + 1] - pb;
             const double num = item_sum<M>(self, np, [&](int j, double &t) {
                 const int2 pr = G.pairs[pb + j];
-                if (!mk.alive(G.U[pr.x] + G.V[pr.x] - u)) return false;
+                if (P.kind == ITEM_DELTA && !edge_live(pr.x, G.U[pr.x] + G.V[pr.x] - u)) return false;
                 t = dadd(dmul(G.w[pr.x], d0[pr.x]), dmul(G.w[pr.y], d0[pr.y]));
                 return true;
             });
@@ -400,7 +415,8 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
 
 __host__ __device__ inline long long group_bytes(const BatchLaunch &L)
 {
-    long long b = 8LL * (2LL * L.maxE + L.maxN) + 8LL * 2 * (L.gsize / 32) + 4LL * (L.maxk > 0 ? L.maxk : 1) + 16;
+    long long b = 8LL * (2LL * L.maxE + L.maxN) + 8LL * 2 * (L.gsize / 32) + 4LL * (L.maxk > 0 ? L.maxk : 1) + 16 +
+                  4LL * ((L.maxE + 31) / 32);       // live-edge bits
     return pl_align(b);
 }
 
@@ -439,6 +455,7 @@ __global__ void __launch_bounds__(GROUP ? 256 : 512, MINB) k_batch(BatchLaunch L
     double *red = vd + L.maxN;
     unsigned long long *slot = (unsigned long long *)(red + 2 * (L.gsize / 32));
     int *ks = (int *)(slot + 2);
+    unsigned *eb = (unsigned *)(ks + (L.maxk > 0 ? L.maxk : 1));
     if (GROUP) {
         for (;;) {
             if (g.t == 0) slot[0] = (unsigned long long)atomicAdd(L.chunk_counter, 1);
@@ -450,7 +467,7 @@ __global__ void __launch_bounds__(GROUP ? 256 : 512, MINB) k_batch(BatchLaunch L
             const ParentDesc P = L.parents[ch.parent];
             const ParentLayout PL = parent_layout(P.N, P.E, P.S, P.T, P.has_nw, P.has_dinit);
             const View G = view_of(P.data, PL, P);
-            for (int i = 0; i < ch.count; ++i) fit_item<M>(P, G, ch.first + i, g, d0, d1, vd, red, ks, slot);
+            for (int i = 0; i < ch.count; ++i) fit_item<M>(P, G, ch.first + i, g, d0, d1, vd, red, ks, slot, eb);
         }
         return;
     }
@@ -478,7 +495,7 @@ __global__ void __launch_bounds__(GROUP ? 256 : 512, MINB) k_batch(BatchLaunch L
             const int item = (int)slot[0];
             g.sync();
             if (item >= ch.count) break;
-            fit_item<M>(P, G, ch.first + item, g, d0, d1, vd, red, ks, slot);
+            fit_item<M>(P, G, ch.first + item, g, d0, d1, vd, red, ks, slot, eb);
         }
         __syncthreads();
     }
@@ -546,7 +563,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_fit_cluster(const ParentDesc 
                          (double *const *)(tab + 3 * CL_MAX_CTAS), nc};
     const DArr d0{tab + 0 * CL_MAX_CTAS, CL_LB, lnc}, d1{tab + 1 * CL_MAX_CTAS, CL_LB, lnc},
         vd{tab + 2 * CL_MAX_CTAS, CL_LB, lnc};
-    fit_item<M>(P, G, 0, g, d0, d1, vd, nullptr, nullptr, nullptr);
+    fit_item<M>(P, G, 0, g, d0, d1, vd, nullptr, nullptr, nullptr, nullptr);
     cl.sync();                                      // no CTA leaves while others read its memory
 }
 
