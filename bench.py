@@ -439,13 +439,18 @@ def bench_k2(args, clocks):
         b.close()
     out["clocks"] = clocks.stop()
     # end to end through the C ABI on a sample of 4 graphs (a full step's
-    # histograms are ~20 GB of host memory)
+    # histograms are ~20 GB of host memory); the first call, untimed, pins
+    # the 1.25 GB staging buffer and grows the device pool, as the headline's
+    # untimed first end-to-end call does
+    res = db.hist_requests(objs[:4], db.DELTA, 2)
+    del res
     t0 = time.perf_counter()
     res = db.hist_requests(objs[:4], db.DELTA, 2)
     dt = time.perf_counter() - t0
     out["delta2"]["e2e_sample"] = {"value": sum(r[3] for r in res) / dt, "unit": "subgraph-fits/s",
-                                   "sample": "first 4 of the 64 graphs, one dressx_hist_batch call",
-                                   "distinct_values": int(sum(r[0].size // 2 for r in res))}
+                                   "sample": "first 4 of the 64 graphs, one dressx_hist_batch call after an untimed one",
+                                   "seconds": dt, "distinct_values": int(sum(r[0].size // 2 for r in res))}
+    del res
     # CPU: the reference's single-thread strided call on graph 0, extrapolated
     import oracle
     cpu = oracle.reference()
