@@ -10,7 +10,9 @@ subgraph fits plus the 2,000 histograms.  Metric: subgraph-fits/s.
   the fits + histograms from CUDA events on the engine stream, L2 flushed
   (256 MiB write) between timed steps, outside the timed regions.
 * ``e2e``: the public C-ABI call ``dressx_hist_batch`` with host graphs,
-  wall clock per step: host packing, H2D, fits, histograms, D2H, results.
+  wall clock per step: host packing, H2D, fits, histograms, D2H, results
+  in malloc'd host arrays.  The caller frees the previous step's arrays
+  before the step's timer starts.
 * ``per_fit_gpu``: the reference's driver structure with this engine's GPU
   fit (``dressx_hist_batch_per_fit``: host subgraph build + one fit launch
   sequence per subgraph) on a bounded sample -- the batched/per-fit ratio.
@@ -249,7 +251,9 @@ def bench_delta1(args, rank, world, pg, torch, clocks):
     # ---- end to end through the C ABI, host graphs ---------------------------
     db.counters(reset=True)
     e2e_s = 0.0
+    out = None
     for step in range(args.steps + 1):
+        out = None                 # the caller releases the previous step's histograms before the timer starts
         t0 = time.perf_counter()
         out = db.hist_requests(objs, db.DELTA, 1, max_iterations=100, epsilon=1e-6)
         dt = time.perf_counter() - t0
