@@ -193,3 +193,25 @@ def test_autotuned_and_captured_batch_matches(kind, k):
     b.close()
     for g in objs:
         g.close()
+
+
+def test_large_batch_download_paths(oracle_port):
+    """A batch whose histogram bound passes 64 MB: the host arrays are mapped
+    while the fits run and the download is split across host threads; the
+    histograms equal the prepared batch's (a separate download path) and,
+    for a few graphs, the oracle's."""
+    gs = graphs.regular_batch(300, (80, 100), (10, 12), seed=21)
+    objs = [db.Graph(n, U, V) for n, U, V in gs]
+    bound = sum(2 * n * len(U) * 8 for n, U, _ in gs)
+    assert bound > 64 << 20
+    direct = [r[0] for r in db.hist_requests(objs, db.DELTA, 1)]
+    b = db.Batch(objs, db.DELTA, 1)
+    b.run()
+    for x, y in zip(direct, b.fetch()):
+        np.testing.assert_array_equal(x, y)
+    b.close()
+    for i in (0, 137, 299):
+        n, U, V = gs[i]
+        np.testing.assert_array_equal(direct[i], oracle_port.delta_fit(n, U, V, k=1)["hist"])
+    for g in objs:
+        g.close()

@@ -211,3 +211,17 @@ def test_cancel_and_bad_requests():
             req.graph = small.ptr
             code = db.lib().dressx_server_submit(srv.handle, db.ctypes.byref(req))
             assert code == EINVAL and req.done == 1 and req.status == EINVAL
+
+
+def test_served_large_histogram_equals_direct_call():
+    """A served Delta^2 request whose one histogram (about 300 MB) a finisher
+    copies out in parts across host threads: the same exact pairs as the
+    direct call."""
+    n, U, V = graphs.random_regular(200, 10, seed=4)
+    with db.Graph(n, U, V) as g:
+        direct = db.hist_requests([g], db.DELTA, 2)[0][0]
+        with db.Server() as srv:
+            r = srv.submit(g, db.DELTA, 2).wait(timeout_ms=600_000)
+        assert r["status"] == 0
+        np.testing.assert_array_equal(r["hist_flat"], direct)
+        assert direct.size * 8 > 64 << 20
