@@ -1,6 +1,6 @@
 """Benchmark of the B200 DRESS engine (one JSON line on rank 0).
 
-Headline workload (BASELINE config "batched Delta^1"): 2,000 random
+Headline workload (batched Delta^1): 2,000 random
 d-regular graphs (configuration model with switching repair), n ~ U[16,100],
 d ~ U{3..12}, unweighted, k = 1, epsilon 1e-6, max 100 sweeps, exact
 (value, count) histogram per graph.  One step = all ~115K vertex-deleted
@@ -18,14 +18,14 @@ subgraph fits plus the 2,000 histograms.  Metric: subgraph-fits/s.
   sequence per subgraph) on a bounded sample -- the batched/per-fit ratio.
 * ``cpu_baseline``: the reference's single-thread C ``dress_delta_fit``
   (compiled from its sources into oracle/_ref) on a bounded sample.
-* ``single_fit``: the 28M-edge Chung-Lu fit (BASELINE config "single large
-  fit"), edge-iters/s and the HBM roofline of its sweeps.
+* ``single_fit``: the 28M-edge Chung-Lu fit (the single large fit),
+  edge-iters/s and the HBM roofline of its sweeps.
 * ``delta2_nabla1``: Delta^2 and Nabla^1 of 64 random 10-regular graphs of
-  200 vertices (BASELINE config 4), autotuned and replayed from a CUDA graph.
-* ``plain_fit``: one G(2000, 10000) fit through
+  200 vertices, autotuned and replayed from a CUDA graph.
+* ``plain_fit``: one G(2000, 10000) fit (the plain fit) through
   dress_fit_cuda and through the server's batch path.
-* ``serving``: a stream of fit and Delta^1 requests (BASELINE config
-  "serving stream") submitted to the request server at Poisson arrival rates
+* ``serving``: a stream of fit and Delta^1 requests (the serving stream)
+  submitted to the request server at Poisson arrival rates
   swept over ``--serve-rates``: graphs/s, subgraph-fits/s, p50/p99 latency
   per request kind and per path, device overlap, admission statistics, a
   spot check that served results equal the same requests run alone, and the
