@@ -1,4 +1,4 @@
-"""CPU parity checker for the B200 DRESS engine (test infrastructure only).
+"""CPU oracle of the B200 DRESS engine's parity tests (test infrastructure only).
 
 Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` import this package.  It wraps two CPU implementations behind
