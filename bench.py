@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-fit workload")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-rates", default="20,80,320", help="Poisson arrival rates (requests/s) to sweep")
+    ap.add_argument("--detail", default="", help="also write every measured figure to this JSON file")
+    ap.add_argument("--no-parity", action="store_true", help="skip the comparisons with the reference")
     return ap.parse_args()
 
 
@@ -302,8 +304,57 @@ def bench_delta1(args, rank, world, pg, torch, clocks):
                 hist_ms=hist_ms / args.steps, wall_ms=wall * 1e3 / args.steps, launches=launches,
                 e2e={"value": e2e_value, "unit": "subgraph-fits/s", "h2d_bytes_per_step": int(h2d_step),
                      "d2h_bytes_per_step": int(d2h_step), "matches_device_run": bool(same)},
-                per_fit=per_fit, roofline=roofline, clocks=clk, gs=gs_all,
+                per_fit=per_fit, roofline=roofline, clocks=clk, gs=gs_all, hists=ref_hist, mine=mine,
                 tune={"threads_per_subgraph": tune[0], "ctas_per_sm": tune[1]})
+
+
+# ---------------------------------------------------------------------------
+# parity with the reference, outside every timed region
+# ---------------------------------------------------------------------------
+
+def ref_cpu():
+    """The reference library compiled from its sources (oracle/_ref), else the
+    oracle's C restatement; the second value names which."""
+    import oracle
+    cpu = oracle.reference()
+    return (cpu, "reference") if cpu is not None else (oracle.port(), "port")
+
+
+def parity_hists(pairs, kind, k):
+    """Histograms of this engine against the reference's call on the same
+    graph: pairs is [((n, U, V), flat [bits, count] array)]."""
+    cpu, which = ref_cpu()
+    omp = which == "reference"
+    fn = cpu.delta_fit if kind == "delta" else cpu.nabla_fit
+    t0 = time.perf_counter()
+    bad = 0
+    for (n, U, V), flat in pairs:
+        ref = fn(n, U, V, k=k, max_iterations=100, epsilon=1e-6, omp=omp)
+        bad += not np.array_equal(flat, ref["hist"])
+    name = f"dress_{kind}_fit" + ("_omp" if omp else " (oracle port)")
+    return {"graphs": len(pairs), "identical": bad == 0, "mismatched": bad, "against": name,
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
+def sha256(a):
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def golden_large(n, U, V, W):
+    """The reference's digests of the single-fit workload
+    (tests/golden/large_fit.json, made by tests/golden/make_large_golden.py),
+    when this run generated the same graph; else None."""
+    path = os.path.join(ROOT, "tests", "golden", "large_fit.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        gold = json.load(f)
+    gg = gold["graph"]
+    if (gg["N"], gg["E"]) != (n, len(U)) or gg["sha_U"] != sha256(U) or gg["sha_V"] != sha256(V) \
+            or gg["sha_W"] != sha256(W):
+        return None
+    return gold
 
 
 # ---------------------------------------------------------------------------
@@ -341,6 +392,7 @@ def bench_single_fit(args, torch):
         out["graph_build"] = {"host_ms": host_ms, "device_ms": dev_ms, "identical": bool(same),
                               "note": "dress_init_graph (host, stable counting sorts) vs dressx_init_graph (GPU radix "
                                       "sort), both including the copies of the caller's arrays in and the CSR out"}
+    gold = None if args.no_parity else golden_large(n, U, V, graphs.uniform_weights(E, seed=7))
     for label, W in (("weighted", graphs.uniform_weights(E, seed=7)), ("unweighted", None)):
         if label not in variants:
             continue
@@ -367,6 +419,15 @@ def bench_single_fit(args, torch):
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
                          "algorithmic_bytes_per_sweep": b_iter},
         }
+        if gold is not None and label in gold:
+            f = gold[label]["full"]
+            out[label]["parity"] = {
+                "ref_iterations": f["iterations"],
+                "identical": bool(it == f["iterations"] and int(np.float64(dl).view(np.int64)) == f["delta_bits"]
+                                  and sha256(g.edge_dress) == f["sha_edge_dress"]
+                                  and sha256(g.vertex_dress) == f["sha_vertex_dress"]),
+                "against": "SHA-256 of the reference's dress_fit_omp edge and vertex values "
+                           "(tests/golden/large_fit.json)"}
         g.close()
     if not args.single_fit_only:
         # the reference's CPU fits on the same weighted graph, a bounded number
@@ -412,6 +473,7 @@ def bench_k2(args, clocks):
                        "autotuned threads per subgraph, fit stage replayed from a CUDA graph",
            "l2": "values of a step (10 GB for Delta^2) exceed L2; parents are staged in shared memory"}
     clocks.start()
+    nabla_hists = None
     for label, kind, k in (("delta2", db.DELTA, 2), ("nabla1", db.NABLA, 1)):
         b = db.Batch(objs, kind, k)
         t0 = time.perf_counter()
@@ -440,6 +502,8 @@ def bench_k2(args, clocks):
                          "sampled_fits_per_ms": {f"{t}x{c}": v for (t, c), v in rates.items()}, "seconds": tune_s},
             "cuda_graph": True,
         }
+        if label == "nabla1" and not args.no_parity:
+            nabla_hists = b.fetch()
         b.close()
     out["clocks"] = clocks.stop()
     # end to end through the C ABI on a sample of 4 graphs (a full step's
@@ -454,6 +518,9 @@ def bench_k2(args, clocks):
     out["delta2"]["e2e_sample"] = {"value": sum(r[3] for r in res) / dt, "unit": "subgraph-fits/s",
                                    "sample": "first 4 of the 64 graphs, one dressx_hist_batch call after an untimed one",
                                    "seconds": dt, "distinct_values": int(sum(r[0].size // 2 for r in res))}
+    if not args.no_parity:
+        out["parity"] = {"delta2": parity_hists(list(zip(gs[:4], [r[0] for r in res])), "delta", 2),
+                         "nabla1": parity_hists(list(zip(gs, nabla_hists)), "nabla", 1)}
     del res
     # CPU: the reference's single-thread strided call on graph 0, extrapolated
     import oracle
@@ -712,6 +779,49 @@ def reference_arm(args, rank):
 
 
 # ---------------------------------------------------------------------------
+# the figures of the other workloads that go on the one JSON line (all of
+# them go to --detail)
+# ---------------------------------------------------------------------------
+
+def _r(x, nd=3):
+    return None if x is None else float(f"{x:.{nd}g}")
+
+
+def compact_sections(single, serving, k2, plain):
+    out = {}
+    if single:
+        sf = {}
+        for label in ("weighted", "unweighted"):
+            v = single.get(label)
+            if v:
+                sf[label] = {"sweep_ms": _r(v["sweep_ms"]), "hbm_frac": _r(v["roofline"]["frac"]),
+                             "edge_iters_per_s": _r(v["edge_iters_per_s"]), "iterations": v["iterations"],
+                             "setup_ms": _r(v["setup_ms"]), "e2e_ms": _r(v["e2e_ms"])}
+                if v["roofline"].get("traffic"):
+                    sf[label]["traffic_gb"] = _r(v["roofline"]["traffic"] / 1e9)
+        cb = single.get("cpu_baseline", {}).get("omp")
+        if cb:
+            sf["cpu_omp_ms_per_sweep"] = _r(cb["ms_per_sweep"])
+        out["single_fit"] = sf
+    if k2:
+        out["delta2_nabla1"] = {lab: {"value": _r(k2[lab]["value"]),
+                                      "schedule": f"{k2[lab]['autotune']['threads_per_subgraph']}x"
+                                                  f"{k2[lab]['autotune']['ctas_per_sm']}",
+                                      "cpu_1t": _r(k2[lab]["cpu_baseline"]["value"])}
+                                for lab in ("delta2", "nabla1")}
+    if plain:
+        cb = plain.get("cpu_baseline", {})
+        out["plain_fit"] = {"ms_per_fit": _r(plain["dress_fit_cuda"]["ms_per_fit"]),
+                            "cpu_1t_ms": _r(1e3 / cb["single_thread"]["value"]) if "single_thread" in cb else None,
+                            "cpu_omp_ms": _r(1e3 / cb["omp"]["value"]) if "omp" in cb else None}
+    if serving:
+        out["serving"] = [{"rate": r["offered_rate"], "graphs_per_s": _r(r["graphs_per_s"]),
+                           "p50_ms": _r(r["p50_ms"]), "p99_ms": _r(r["p99_ms"]), "failed": r["failed"]}
+                          for r in serving["rates"]]
+    return out
+
+
+# ---------------------------------------------------------------------------
 
 def main():
     args = parse()
@@ -747,26 +857,50 @@ def main():
             k2 = bench_k2(args, Clocks(local))
         if not args.no_plain:
             plain = bench_plain(args)
+    parity = {}
+    if rank == 0 and not args.no_parity:
+        # every graph this rank fitted, against the reference's OpenMP Delta^1
+        parity["delta1"] = parity_hists(list(zip(head["mine"], head["hists"])), "delta", 1)
+        if k2 and "parity" in k2:
+            parity.update(k2["parity"])
+        if single:
+            for label in ("weighted", "unweighted"):
+                pr = (single.get(label) or {}).get("parity")
+                if pr:
+                    parity[f"single_fit_{label}"] = {"identical": pr["identical"],
+                                                     "ref_iterations": pr["ref_iterations"]}
     if rank == 0:
         clk = head["clocks"]
+        detail = {"headline": {k: v for k, v in head.items() if k not in ("gs", "hists", "mine")},
+                  "cpu_baseline": cpu, "single_fit": single, "serving": serving, "delta2_nabla1": k2,
+                  "plain_fit": plain, "parity": parity}
+        if args.detail:
+            with open(args.detail, "w") as f:
+                json.dump(detail, f, indent=1, default=float)
         line = {
             "metric": "Delta^1 subgraph-fits/s", "value": head["value"], "unit": "subgraph-fits/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"batched Delta^1 of {args.graphs} random d-regular graphs "
-                                   "(configuration model + switching repair, n~U[16,100], d~U{3..12}, seed 42), "
-                                   "k=1, epsilon 1e-6, max 100 sweeps, exact histogram per graph",
-                       "fits_per_step": head["fits_per_step"], "edge_updates_per_step": head["edge_updates_per_step"],
-                       "l2": "256 MiB flush between timed steps (outside the timed regions)",
+            "config": {"workload": f"batched Delta^1 of {args.graphs} random d-regular graphs (n~U[16,100], "
+                                   "d~U{3..12}, seed 42), k=1, epsilon 1e-6, exact histogram per graph",
+                       "fits_per_step": head["fits_per_step"],
+                       "l2": "256 MiB flush between timed steps",
                        "parallelism": f"graphs sharded over {world} GPU(s)",
-                       "schedule": head["tune"]},
+                       "schedule": f"{head['tune']['threads_per_subgraph']} threads/subgraph, "
+                                   f"{head['tune']['ctas_per_sm']} CTA/SM"},
             "e2e": head["e2e"], "gpu_launches": head["launches"], "roofline": head["roofline"],
-            "cpu_baseline": cpu, "per_fit_gpu": head["per_fit"],
-            "breakdown_ms": {"fits": head["fit_ms"], "histograms": head["hist_ms"], "wall": head["wall_ms"]},
-            "clocks": clk, "single_fit": single, "serving": serving, "delta2_nabla1": k2, "plain_fit": plain,
+            "cpu_baseline": cpu, "clocks": clk,
+            "breakdown_ms": {"fits": head["fit_ms"], "histograms": head["hist_ms"]},
         }
-        print(json.dumps(line), flush=True)
+        if head["per_fit"]:
+            line["per_fit_gpu"] = {"value": head["per_fit"]["value"],
+                                   "batched_over_per_fit": head["per_fit"]["batched_over_per_fit"]}
+        line.update(compact_sections(single, serving, k2, plain))
+        if parity:
+            line["parity"] = {k: {"graphs": v["graphs"], "identical": v["identical"]} if "graphs" in v else v
+                              for k, v in parity.items()}
+        print(json.dumps(line, default=float), flush=True)
     if pg is not None:
         barrier(pg)
         pg.destroy_process_group()

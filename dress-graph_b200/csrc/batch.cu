@@ -27,95 +27,61 @@ namespace cg = cooperative_groups;
 namespace dress {
 namespace {
 
-__device__ __forceinline__ void cmx(double &a, double &b)
+// The exact sorted KBN of the self term (index cnt) and the live stored
+// terms, visited in ascending (value, index) order by repeated scans: no
+// storage, O(cnt^2) term evaluations.  Equal values are interchangeable in
+// the sum, so this is the reference's "sort, then KBN" (dress.c:51-66).  It
+// runs only for the items whose certified sum fails (about one in 1e9).
+template <class Terms>
+__device__ __noinline__ double sorted_sum_select(double self, int cnt, Terms term)
 {
-    double lo = fmin(a, b), hi = fmax(a, b);
-    a = lo;
-    b = hi;
-}
-
-// Bitonic network (single-direction form) on the first m registers, without
-// the comparators whose upper slot is S or beyond: slots from S on hold
-// +inf, and every comparator keeps the larger value in its upper slot, so
-// those slots never change and their comparators do nothing.
-template <int m, int S, int M>
-__device__ __forceinline__ void net(double (&a)[M])
-{
-#pragma unroll
-    for (int k = 2; k <= m; k <<= 1) {
-#pragma unroll
-        for (int i = 0; i < m; ++i) {
-            int j = i ^ (k - 1);
-            if (j > i && j < S) cmx(a[i], a[j]);
-        }
-#pragma unroll
-        for (int s = k >> 2; s > 0; s >>= 1) {
-#pragma unroll
-            for (int i = 0; i < m; ++i) {
-                int j = i ^ s;
-                if (j > i && j < S) cmx(a[i], a[j]);
+    double pv = -DRESS_INF, s = 0.0, c = 0.0;
+    int pj = -1;
+    bool first = true;
+    for (;;) {
+        double bv = DRESS_INF;
+        int bj = INT_MAX;
+        for (int j = 0; j <= cnt; ++j) {
+            double t = self;
+            if (j < cnt && !term(j, t)) continue;
+            const bool after = t > pv || (t == pv && j > pj);
+            const bool better = t < bv || (t == bv && j < bj);
+            if (after && better) {
+                bv = t;
+                bj = j;
             }
         }
-    }
-}
-
-// Sorted KBN of the self term and the live ones among cnt stored terms
-// (term(j, t) yields stored term j and whether it is alive) in a register
-// network of Mi > cnt slots, of which the first S are used (S = cnt + 1
-// when known at compile time, else Mi); dead and unused slots hold +inf.
-template <int Mi, int S, class Term>
-__device__ __forceinline__ double net_sum(double self, int cnt, Term term)
-{
-    double a[Mi];
-    a[0] = self;
-    int n = 1;
-#pragma unroll
-    for (int j = 1; j < Mi; ++j) {
-        a[j] = DRESS_INF;
-        if (j < S && j <= cnt) {
-            double t;
-            if (term(j - 1, t)) {
-                a[j] = t;
-                ++n;
-            }
+        if (bj == INT_MAX) break;
+        if (first) {
+            s = bv;
+            first = false;
+        } else {
+            kbn_step(s, c, bv);
         }
+        pv = bv;
+        pj = bj;
     }
-    net<Mi, S, Mi>(a);
-    double s = a[0], c = 0.0;
-#pragma unroll
-    for (int i = 1; i < Mi; ++i)
-        if (i < n) kbn_step(s, c, a[i]);
     return dadd(s, c);
 }
 
-// Networks of 2, 4, 6, 8, 10, 12, 14 and 16 slots (the comparators of the
-// unused tail dropped), the full M-slot network beyond.  A few sizes only:
-// the warps of an SM fit subgraphs of different degrees at once, and one
-// network per slot count measured slower on such batches (instruction
-// cache): on 2,000 regular graphs of degree 3-12, 29.6 ms against 24.6 ms
-// with these eight and 25.2 ms with six (no 10, 14).
-template <int M, class Term>
-__device__ __forceinline__ double sum_pruned(double self, int cnt, Term term)
+// Sum of the self term and the live ones among cnt stored terms (term(j, t)
+// yields stored term j and whether it is alive): a certified sum in stored
+// order (CSum, common.cuh), the exact sorted sum where the certificate fails.
+template <class Terms>
+__device__ __forceinline__ double item_sum(double self, int cnt, const Terms &term, bool force_exact)
 {
-    const int S = cnt + 1;
-    if (S <= 2) return net_sum<2, 2>(self, cnt, term);
-    if (M >= 4 && S <= 4) return net_sum<(M >= 4 ? 4 : 2), (M >= 4 ? 4 : 2)>(self, cnt, term);
-    if (M >= 8 && S <= 6) return net_sum<(M >= 8 ? 8 : 2), (M >= 8 ? 6 : 2)>(self, cnt, term);
-    if (M >= 8 && S <= 8) return net_sum<(M >= 8 ? 8 : 2), (M >= 8 ? 8 : 2)>(self, cnt, term);
-    if (M >= 16 && S <= 10) return net_sum<(M >= 16 ? 16 : 2), (M >= 16 ? 10 : 2)>(self, cnt, term);
-    if (M >= 16 && S <= 12) return net_sum<(M >= 16 ? 16 : 2), (M >= 16 ? 12 : 2)>(self, cnt, term);
-    if (M >= 16 && S <= 14) return net_sum<(M >= 16 ? 16 : 2), (M >= 16 ? 14 : 2)>(self, cnt, term);
-    if (M >= 16 && S <= 16) return net_sum<(M >= 16 ? 16 : 2), (M >= 16 ? 16 : 2)>(self, cnt, term);
-    return net_sum<M, M>(self, cnt, term);
-}
-
-// The smallest network that holds the item: most items of sparse subgraphs
-// have a handful of terms, and the cost of a network grows with its size.
-template <int M, class Term>
-__device__ __forceinline__ double item_sum(double self, int cnt, Term term)
-{
-    if (cnt == 0) return dadd(self, 0.0);
-    return sum_pruned<M>(self, cnt, term);
+    if (cnt == 0) return dadd(self, 0.0);        // one term: the reference's sum + comp
+    if (force_exact) return sorted_sum_select(self, cnt, term);
+    CSum q;
+    q.init();
+    q.add(self);
+    for (int j = 0; j < cnt; ++j) {
+        double t;
+        if (term(j, t)) q.add(t);
+    }
+    double r;
+    if (q.result(r)) return r;
+    return sorted_sum_select(self, cnt, term);
 }
 
 __device__ __forceinline__ long long binom_d(int n, int k)
@@ -262,10 +228,48 @@ __device__ __forceinline__ int group_sum(const ClusterGroup &g, int v, double *,
     return (int)cluster_reduce(g, (double)v, parity, [](double a, double b) { return a + b; });
 }
 
-// eb (nullable): E bits of group memory, set for the live edges of a Delta
-// subgraph; with them a term's liveness is one bit instead of its endpoints'
-// lookup against the deleted vertices.
-template <int M, class Grp, class Arr>
+// Stored terms of vertex u's row, w[e] d[e] of every live slot edge
+// (dress.c:566-569).  eb (nullable): E bits of group memory, set for the live
+// edges of a Delta subgraph; with them a term's liveness is one bit instead
+// of its endpoints' lookup against the deleted vertices.
+template <class Arr>
+struct RowTerms {
+    View G;
+    Mask mk;
+    Arr d0;
+    const unsigned *eb;
+    int rb, u;
+    bool delta;
+    __device__ __forceinline__ bool operator()(int j, double &t) const
+    {
+        const int e = G.row_eid[rb + j];
+        if (delta && !(eb ? ((eb[e >> 5] >> (e & 31)) & 1u) != 0 : mk.alive(G.U[e] + G.V[e] - u))) return false;
+        t = dmul(G.w[e], d0[e]);
+        return true;
+    }
+};
+
+// Common-neighbour terms of edge (u, v): w[eu] d[eu] + w[ev] d[ev] of every
+// pair whose (u, x) edge is live (dress.c:485-490)
+template <class Arr>
+struct PairTerms {
+    View G;
+    Mask mk;
+    Arr d0;
+    const unsigned *eb;
+    int pb, u;
+    bool delta;
+    __device__ __forceinline__ bool operator()(int j, double &t) const
+    {
+        const int2 pr = G.pairs[pb + j];
+        if (delta && !(eb ? ((eb[pr.x >> 5] >> (pr.x & 31)) & 1u) != 0 : mk.alive(G.U[pr.x] + G.V[pr.x] - u)))
+            return false;
+        t = dadd(dmul(G.w[pr.x], d0[pr.x]), dmul(G.w[pr.y], d0[pr.y]));
+        return true;
+    }
+};
+
+template <class Grp, class Arr>
 __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
                          const Grp &g, Arr d0, Arr d1, Arr vd, double *red, int *ks,
                          unsigned long long *slot, unsigned *eb)
@@ -318,10 +322,6 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
     }
     g.sync();                                    // the bits and initial values, group-wide
     live = group_sum(g, live, red, 0);
-    // is edge e live (given one of its endpoints is)
-    auto edge_live = [&](int e, int other) {
-        return bits ? ((eb[e >> 5] >> (e & 31)) & 1u) != 0 : mk.alive(other);
-    };
     if (live == 0 && P.kind != ITEM_PLAIN) {   // the reference skips edgeless subgraphs
         g.sync();
         return;
@@ -334,12 +334,8 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
         for (int u = g.t; u < N; u += g.size) {
             if (!mk.alive(u)) continue;
             const int rb = G.row_off[u], deg = G.row_off[u + 1] - rb;
-            vd[u] = dsqrt(item_sum<M>(dmul(4.0, mk.weight(u, G.nw)), deg, [&](int j, double &t) {
-                const int e = G.row_eid[rb + j];
-                if (P.kind == ITEM_DELTA && !edge_live(e, G.U[e] + G.V[e] - u)) return false;
-                t = dmul(G.w[e], d0[e]);
-                return true;
-            }));
+            const RowTerms<Arr> rt{G, mk, d0, bits ? eb : nullptr, rb, u, P.kind == ITEM_DELTA};
+            vd[u] = dsqrt(item_sum(dmul(4.0, mk.weight(u, G.nw)), deg, rt, P.force_exact != 0));
         }
         g.sync();
         double lmax = 0.0;
@@ -351,12 +347,8 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
             const double a4u = dmul(4.0, mk.weight(u, G.nw));
             const double self = P.fwd ? dadd(a4u, own) : dadd(dadd(a4u, dmul(4.0, mk.weight(v, G.nw))), dmul(2.0, own));
             const int pb = G.ioff[e], np = G.ioff[e + 1] - pb;
-            const double num = item_sum<M>(self, np, [&](int j, double &t) {
-                const int2 pr = G.pairs[pb + j];
-                if (P.kind == ITEM_DELTA && !edge_live(pr.x, G.U[pr.x] + G.V[pr.x] - u)) return false;
-                t = dadd(dmul(G.w[pr.x], d0[pr.x]), dmul(G.w[pr.y], d0[pr.y]));
-                return true;
-            });
+            const PairTerms<Arr> pt{G, mk, d0, bits ? eb : nullptr, pb, u, P.kind == ITEM_DELTA};
+            const double num = item_sum(self, np, pt, P.force_exact != 0);
             const double den = dmul(vd[u], vd[v]);
             const double r = den > 0.0 ? ddiv(num, den) : 0.0;
             d1[e] = r;
@@ -441,7 +433,7 @@ __device__ __forceinline__ View view_of(const unsigned char *b, const ParentLayo
 // own and reads the parent through L2, so no group idles behind another.
 // Group-mode CTAs hold at most 256 threads (several per SM), which leaves
 // the register budget of the larger networks unsplit.
-template <int M, bool GROUP, int MINB>
+template <bool GROUP, int MINB>
 __global__ void __launch_bounds__(GROUP ? 256 : 512, MINB) k_batch(BatchLaunch L)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -467,7 +459,7 @@ __global__ void __launch_bounds__(GROUP ? 256 : 512, MINB) k_batch(BatchLaunch L
             const ParentDesc P = L.parents[ch.parent];
             const ParentLayout PL = parent_layout(P.N, P.E, P.S, P.T, P.has_nw, P.has_dinit);
             const View G = view_of(P.data, PL, P);
-            for (int i = 0; i < ch.count; ++i) fit_item<M>(P, G, ch.first + i, g, d0, d1, vd, red, ks, slot, eb);
+            for (int i = 0; i < ch.count; ++i) fit_item(P, G, ch.first + i, g, d0, d1, vd, red, ks, slot, eb);
         }
         return;
     }
@@ -495,38 +487,36 @@ __global__ void __launch_bounds__(GROUP ? 256 : 512, MINB) k_batch(BatchLaunch L
             const int item = (int)slot[0];
             g.sync();
             if (item >= ch.count) break;
-            fit_item<M>(P, G, ch.first + item, g, d0, d1, vd, red, ks, slot, eb);
+            fit_item(P, G, ch.first + item, g, d0, d1, vd, red, ks, slot, eb);
         }
         __syncthreads();
     }
 }
 
-template <int M, bool GROUP, int MINB>
+template <bool GROUP, int MINB>
 Status launch_mg(const BatchLaunch &L, int sms, cudaStream_t st)
 {
     if (GROUP && L.gsize * L.groups > 256)
         return Status::Err(DRESSX_EINVAL, "group-mode batch CTAs hold at most 256 threads");
     size_t smem = batch_smem_bytes(L);
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_batch<M, GROUP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_batch<GROUP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    DRESS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<M, GROUP, MINB>, L.gsize * L.groups, smem));
+    DRESS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<GROUP, MINB>, L.gsize * L.groups, smem));
     if (per_sm < 1) return Status::Err(DRESSX_EUNSUPPORTED, "batch kernel does not fit on an SM");
     long long grid = (long long)per_sm * sms;
     // no more CTAs than there are chunks (group mode: chunks per CTA = groups)
     long long need = GROUP ? (L.nchunks + L.groups - 1) / L.groups : L.nchunks;
     if (grid > need) grid = need;
-    count_launch(), k_batch<M, GROUP, MINB><<<(int)grid, L.gsize * L.groups, smem, st>>>(L);
+    count_launch(), k_batch<GROUP, MINB><<<(int)grid, L.gsize * L.groups, smem, st>>>(L);
     DRESS_CUDA_TRY(cudaGetLastError());
     return Status::Ok();
 }
 
-// Two CTAs per SM (64 registers a thread) only where the networks allow it.
-template <int M>
-Status launch_m(const BatchLaunch &L, int sms, cudaStream_t st)
+Status launch_any(const BatchLaunch &L, int sms, cudaStream_t st)
 {
-    if (L.per_group) return launch_mg<M, true, 1>(L, sms, st);
-    if (M <= 16 && L.min_ctas == 2) return launch_mg<M, false, (M <= 16 ? 2 : 1)>(L, sms, st);
-    return launch_mg<M, false, 1>(L, sms, st);
+    if (L.per_group) return launch_mg<true, 1>(L, sms, st);
+    if (L.min_ctas == 2) return launch_mg<false, 2>(L, sms, st);
+    return launch_mg<false, 1>(L, sms, st);
 }
 
 // One whole-graph fit (ParentDesc of kind ITEM_PLAIN) by one cluster of
@@ -536,7 +526,6 @@ Status launch_m(const BatchLaunch &L, int sms, cudaStream_t st)
 constexpr int CL_THREADS = 512, CL_LB = 9;
 constexpr int CL_MAX_CTAS = 16;
 
-template <int M>
 __global__ void __launch_bounds__(CL_THREADS, 1) k_fit_cluster(const ParentDesc *pp, int per_e, int per_n, int lnc)
 {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -563,19 +552,18 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_fit_cluster(const ParentDesc 
                          (double *const *)(tab + 3 * CL_MAX_CTAS), nc};
     const DArr d0{tab + 0 * CL_MAX_CTAS, CL_LB, lnc}, d1{tab + 1 * CL_MAX_CTAS, CL_LB, lnc},
         vd{tab + 2 * CL_MAX_CTAS, CL_LB, lnc};
-    fit_item<M>(P, G, 0, g, d0, d1, vd, nullptr, nullptr, nullptr, nullptr);
+    fit_item(P, G, 0, g, d0, d1, vd, nullptr, nullptr, nullptr, nullptr);
     cl.sync();                                      // no CTA leaves while others read its memory
 }
 
-template <int M>
 Status launch_cluster_m(const ParentDesc *d_parent, int E, int N, int lnc, int sms, cudaStream_t st)
 {
     const int nc = 1 << lnc, span = nc * CL_THREADS;
     const int per_e = ((E + span - 1) / span) * CL_THREADS, per_n = ((N + span - 1) / span) * CL_THREADS;
     const size_t smem = (size_t)(2 * per_e + per_n + 2 * (CL_THREADS / 32) + 2) * sizeof(double) +
                         4 * CL_MAX_CTAS * sizeof(double *);
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (nc > 8) DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster<M>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (nc > 8) DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)nc);
     cfg.blockDim = dim3(CL_THREADS);
@@ -589,12 +577,12 @@ Status launch_cluster_m(const ParentDesc *d_parent, int E, int N, int lnc, int s
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, k_fit_cluster<M>, &cfg) != cudaSuccess || clusters < 1) {
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_fit_cluster, &cfg) != cudaSuccess || clusters < 1) {
         cudaGetLastError();
         return Status::Err(DRESSX_EUNSUPPORTED, "cluster fit does not fit the device");
     }
     count_launch();
-    DRESS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_fit_cluster<M>, d_parent, per_e, per_n, lnc));
+    DRESS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_fit_cluster, d_parent, per_e, per_n, lnc));
     (void)sms;
     return Status::Ok();
 }
@@ -608,17 +596,10 @@ size_t cluster_fit_smem_bytes(int E, int N, int lnc)
     return (size_t)(2 * per_e + per_n + 2 * (CL_THREADS / 32) + 2) * sizeof(double) + 4 * CL_MAX_CTAS * sizeof(double *);
 }
 
-Status launch_cluster_fit(const ParentDesc *d_parent, int E, int N, int M, int lnc, int sms, cudaStream_t st)
+Status launch_cluster_fit(const ParentDesc *d_parent, int E, int N, int lnc, int sms, cudaStream_t st)
 {
     if (lnc < 0 || (1 << lnc) > CL_MAX_CTAS) return Status::Err(DRESSX_EINVAL, "cluster size out of range");
-    switch (M) {
-    case 2: return launch_cluster_m<2>(d_parent, E, N, lnc, sms, st);
-    case 4: return launch_cluster_m<4>(d_parent, E, N, lnc, sms, st);
-    case 8: return launch_cluster_m<8>(d_parent, E, N, lnc, sms, st);
-    case 16: return launch_cluster_m<16>(d_parent, E, N, lnc, sms, st);
-    case 32: return launch_cluster_m<32>(d_parent, E, N, lnc, sms, st);
-    default: return Status::Err(DRESSX_EUNSUPPORTED, "cluster fit network size out of range");
-    }
+    return launch_cluster_m(d_parent, E, N, lnc, sms, st);
 }
 
 long long batch_group_bytes(int maxE, int maxN, int maxk, int gsize)
@@ -639,14 +620,7 @@ size_t batch_smem_bytes(const BatchLaunch &L)
 Status launch_batch(const BatchLaunch &L, int sms, cudaStream_t st)
 {
     if (L.nchunks <= 0) return Status::Ok();
-    switch (L.M) {
-    case 2: return launch_m<2>(L, sms, st);
-    case 4: return launch_m<4>(L, sms, st);
-    case 8: return launch_m<8>(L, sms, st);
-    case 16: return launch_m<16>(L, sms, st);
-    case 32: return launch_m<32>(L, sms, st);
-    default: return Status::Err(DRESSX_EUNSUPPORTED, "batch network size out of range");
-    }
+    return launch_any(L, sms, st);
 }
 
 }  // namespace dress

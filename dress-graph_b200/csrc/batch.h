@@ -57,6 +57,7 @@ struct ParentDesc {
     double *multisets;   // C(N,k) x E row-major matrix, or null
     const long long *ranks;      // sampled ranks (item i -> ranks[i]), or null ...
     long long offset, stride;    // ... else rank of item i = offset + i*stride
+    int force_exact;             // every sum by the exact sorted path (tests of that path)
 };
 
 struct Chunk {
@@ -76,15 +77,14 @@ struct BatchLaunch {
     int min_ctas;                    // CTAs per SM the schedule is built for (1 or 2)
     int maxE, maxN, maxk;            // per-group state sizes
     long long parent_bytes;          // staging area size
-    int M;                           // register network size (max terms)
+    int M;                           // most terms of any item (a row or an edge's pairs, plus one)
 };
 
 Status launch_batch(const BatchLaunch &L, int sms, cudaStream_t st);
 // One whole-graph fit (the ITEM_PLAIN descriptor at d_parent) by one cluster
 // of 2^lnc CTAs whose shared memory holds the state (cluster_fit_smem_bytes
-// per CTA); M is the register network size.  DRESSX_EUNSUPPORTED when such a
-// cluster cannot be placed.
-Status launch_cluster_fit(const ParentDesc *d_parent, int E, int N, int M, int lnc, int sms, cudaStream_t st);
+// per CTA).  DRESSX_EUNSUPPORTED when such a cluster cannot be placed.
+Status launch_cluster_fit(const ParentDesc *d_parent, int E, int N, int lnc, int sms, cudaStream_t st);
 size_t cluster_fit_smem_bytes(int E, int N, int lnc);
 size_t batch_smem_bytes(const BatchLaunch &L);
 // Shared memory of one group's state (edge values twice, vertex norms,

@@ -3,10 +3,10 @@
 // Exactness rules (all kernels are compiled with --fmad=false as well):
 //   * every product and sum uses the explicit round-to-nearest intrinsics,
 //     so no multiply-add is ever fused;
-//   * every multi-term sum is "sort ascending, then sequential
-//     Kahan-Babuska-Neumaier" exactly as the reference does it
-//     (libdress/src/dress.c:51-66), which makes the result independent of
-//     the order in which the terms were gathered;
+//   * every multi-term sum has the bits of "sort ascending, then sequential
+//     Kahan-Babuska-Neumaier" as the reference computes it
+//     (libdress/src/dress.c:51-66): either a certified sum in gathering order
+//     (CSum below) or, where the certificate fails, that sorted sum itself;
 //   * sqrt and division are the IEEE round-to-nearest forms.
 #pragma once
 #include <cuda_runtime.h>
@@ -34,6 +34,106 @@ __device__ __forceinline__ void kbn_step(double &s, double &c, double b)
     c = dadd(c, dadd(dsub(big, t), small));
     s = t;
 }
+
+// ---- certified sums -----------------------------------------------------------
+// The reference sums every item's terms by "sort ascending, then sequential
+// Neumaier" (libdress/src/dress.c:51-66).  CSum adds the same terms in ANY
+// order (or several partial sums merged in any tree) and then decides, per
+// item, whether its result is provably the bits the sorted sum gives:
+//
+//   s  running sum;  c  sum of the exact rounding errors of every addition
+//   into s (Fast2Sum on the larger operand, as the reference's step);
+//   a  sum of |x|;  m  smallest term;  n  number of terms.
+//
+// Whatever the order, s + c equals the exact real sum X of the terms plus
+// the rounding error d of the additions into c.  Each error folded into c is
+// at most u|t| <= u(1+u)^n a  (u = 2^-53), c takes at most 3n roundings
+// (one per term, two per merge), so |d| <= 6.1 n^2 u^2 a for any order -- the
+// sorted order included.  Two ways to prove that the sorted sum rounds to
+// the same double R = fl(s + c):
+//   * exact compensation: all terms positive, every term, partial sum and
+//     error a multiple of q = ulp(m), and 2n u a < 2^53 q bounds every
+//     partial sum of errors, so every addition into c is exact in any order:
+//     d = 0 for both orders, both results are fl(X);
+//   * margin: with rho = (s + c) - R computed exactly, the sorted order's
+//     pre-rounding value lies within |rho| + 2B of R (B = 16 n^2 u^2 a >= |d|);
+//     if that is below the half-gap between R and its nearer neighbour, it
+//     rounds to R as well.
+// Otherwise (R zero, subnormal or not finite, or a value close to a rounding
+// boundary, about 1e-9 of items) result() returns false and the caller sorts.
+struct CSum {
+    double s, c, a, m;
+    int n;
+    __device__ __forceinline__ void init()
+    {
+        s = 0.0;
+        c = 0.0;
+        a = 0.0;
+        m = DRESS_INF;
+        n = 0;
+    }
+    __device__ __forceinline__ void add(double x)
+    {
+        const double t = dadd(s, x);
+        const bool g = fabs(s) >= fabs(x);
+        const double big = g ? s : x, small = g ? x : s;
+        c = dadd(c, dadd(dsub(big, t), small));
+        s = t;
+        a = dadd(a, fabs(x));
+        m = fmin(m, x);
+        ++n;
+    }
+    __device__ __forceinline__ void merge(double os, double oc, double oa, double om, int on)
+    {
+        const double t = dadd(s, os);
+        const bool g = fabs(s) >= fabs(os);
+        const double big = g ? s : os, small = g ? os : s;
+        c = dadd(dadd(c, oc), dadd(dsub(big, t), small));
+        s = t;
+        a = dadd(a, oa);
+        m = fmin(m, om);
+        n += on;
+    }
+    // butterfly over the `width` lanes of a group (all lanes end equal)
+    __device__ __forceinline__ void merge_lanes(int width)
+    {
+        for (int o = width >> 1; o > 0; o >>= 1) {
+            const double os = __shfl_xor_sync(0xffffffffu, s, o);
+            const double oc = __shfl_xor_sync(0xffffffffu, c, o);
+            const double oa = __shfl_xor_sync(0xffffffffu, a, o);
+            const double om = __shfl_xor_sync(0xffffffffu, m, o);
+            const int on = __shfl_xor_sync(0xffffffffu, n, o);
+            merge(os, oc, oa, om, on);
+        }
+    }
+    __device__ __forceinline__ bool result(double &out) const
+    {
+        const double R = dadd(s, c);
+        const unsigned long long b = (unsigned long long)__double_as_longlong(R) & 0x7fffffffffffffffULL;
+        const int ex = (int)(b >> 52);
+        if (ex < 64 || ex > 2000) return false;
+        if (m > 0.0) {
+            const double mp2 = __longlong_as_double(__double_as_longlong(m) & 0x7ff0000000000000LL);
+            if (dmul(dmul((double)n, a), 0x1p-50) < mp2) {
+                out = R;
+                return true;
+            }
+        }
+        // rho = (s + c) - R exactly (Fast2Sum on the larger operand)
+        const bool g = fabs(s) >= fabs(c);
+        const double big = g ? s : c, small = g ? c : s;
+        const double rho = dadd(dsub(big, R), small);
+        double hg = __longlong_as_double((long long)(ex - 53) << 52);
+        if ((b & 0xfffffffffffffULL) == 0) hg = dmul(hg, 0.5);
+        const double nn = (double)n;
+        const double B = dmul(dmul(dmul(nn, nn), 0x1p-102), a);
+        if (dadd(fabs(rho), dmul(2.0, B)) < hg) {
+            out = R;
+            return true;
+        }
+        return false;
+    }
+};
 
 // Compare-exchange putting the smaller value at the lower position.
 __device__ __forceinline__ void cswap(double &a, double &b)

@@ -187,8 +187,9 @@ Status prepare(Prep &p)
     p.M = std::max(2, next_pow2(maxdeg + 1));
     // Masks reproduce the rebuilt subgraph except for the reciprocal-weight
     // lookup of DIRECTED graphs with repeated directed edges.
-    // The batch kernel also needs one subgraph's state in shared memory.
-    p.batchable = p.M <= 32 && !(dup && g->variant == DRESS_VARIANT_DIRECTED) &&
+    // The batch kernel also needs one subgraph's state in shared memory;
+    // rows of any length are summed there (certified sums, no networks).
+    p.batchable = !(dup && g->variant == DRESS_VARIANT_DIRECTED) &&
                   batch_group_bytes(p.E, p.N, k, 32) <= BATCH_GROUP_BYTES_MAX;
     return Status::Ok();
 }
@@ -374,7 +375,7 @@ bool shape_launch(BatchLaunch &L, const Tune &tu, long long smem_cap_full, long 
     // two CTAs per SM split the SM's shared memory (each keeps ~1 KB of
     // system and static shared memory)
     const long long smem_cap = tu.per_sm == 2 && smem_sm > 0 ? smem_sm / 2 - 2048 : smem_cap_full;
-    L.min_ctas = tu.per_sm == 2 && smem_sm > 0 && L.M <= 16 ? 2 : 1;
+    L.min_ctas = tu.per_sm == 2 && smem_sm > 0 ? 2 : 1;
     L.gsize = tu.gsize;
     L.per_group = 0;
     L.stage = 1;
@@ -469,6 +470,7 @@ Status plan_batched(std::vector<Prep *> &ps, const Ctx &en, BatchPlan &P)
         d.kind = p->r->kind == DRESSX_DELTA ? ITEM_DELTA : ITEM_NABLA;
         d.k = p->r->k;
         d.fwd = p->g->variant == DRESS_VARIANT_FORWARD || p->g->variant == DRESS_VARIANT_BACKWARD;
+        d.force_exact = en.cfg->exact_sums != 0;
         d.max_iter = p->r->max_iterations;
         d.eps = p->r->epsilon;
         d.offset = p->r->offset;
@@ -685,9 +687,7 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
     // SM to show the tail of a schedule), a spread quarter beyond
     const long long limit = total <= 200000 ? total : std::max<long long>(200000, total / 4);
     struct Cand { int gs, per_sm; };
-    std::vector<Cand> cands = {{32, 1}, {64, 1}, {128, 1}, {256, 1}};
-    if (P.L.M <= 16)                      // the kernel fits two 512-thread CTAs per SM there
-        for (int gs : {32, 64, 128}) cands.push_back({gs, 2});
+    std::vector<Cand> cands = {{32, 1}, {64, 1}, {128, 1}, {256, 1}, {32, 2}, {64, 2}, {128, 2}};
     DevBuf<Chunk> d_try;
     cudaEvent_t e0, e1;
     DRESS_CUDA_TRY(cudaEventCreate(&e0));

@@ -535,32 +535,6 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         }
     }
 
-    // per-item slots for the sorted terms of the block items (both block bins)
-    DevBuf<long long> d_bofs_v, d_bofs_e;
-    DevBuf<double> d_bkey_v, d_bkey_e;
-    {
-        struct Blk { int *perm; const int *len; int b0, b1; DevBuf<long long> *ofs; DevBuf<double> *keys; };
-        Blk blks[2] = {{d_vperm.get(), d_deg.get(), vb.start[BBLOCK], vb.start[BBIG + 1], &d_bofs_v, &d_bkey_v},
-                       {d_eperm.get(), d_cnt.get(), eb.start[BBLOCK], eb.start[BBIG + 1], &d_bofs_e, &d_bkey_e}};
-        for (Blk &k : blks) {
-            const int n = k.b1 - k.b0;
-            DRESS_TRY(k.ofs->alloc((size_t)n + 1, st));
-            std::vector<long long> ofs((size_t)n + 1, 0);
-            if (n > 0) {
-                DevBuf<int> d_len;
-                DRESS_TRY(d_len.alloc((size_t)n, st));
-                count_launch(), k_gather_seg<<<grid_for(n, 256, 64 * sms), 256, 0, st>>>(n, k.perm + k.b0, k.len, d_len.get());
-                std::vector<int> len((size_t)n);
-                DRESS_CUDA_TRY(counted_memcpy(len.data(), d_len.get(), (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st));
-                DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-                for (int i = 0; i < n; ++i) ofs[(size_t)i + 1] = ofs[(size_t)i] + len[(size_t)i];
-            }
-            DRESS_CUDA_TRY(counted_memcpy(k.ofs->get(), ofs.data(), ((size_t)n + 1) * sizeof(long long),
-                                          cudaMemcpyHostToDevice, st));
-            DRESS_TRY(k.keys->alloc((size_t)(ofs[(size_t)n] > 0 ? ofs[(size_t)n] : 1), st));
-        }
-    }
-
     DevBuf<int> d_ndeg, d_row_eid, d_eu, d_ev, d_ncnt;
     DevBuf<long long> d_row_off, d_ioff;
     DevBuf<double> d_nwi, d_wi, d_dbuf, d_pbuf, d_vd;
@@ -598,25 +572,22 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     d_U.release(); d_V.release(); d_w.release(); d_d.release(); d_nw.release();
     d_pairs_old.release(); d_ioff_old.release(); d_ncnt.release(); d_cnt.release(); d_deg.release();
 
-    // block-bin shared memory and spill area
+    // exact sums of queued items: shared memory for their terms, a global
+    // scratch slice per block for items beyond it
     int smem_optin = 0;
     DRESS_CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx.device));
-    // keys (8 B) and payload (8 B edge pair, 4 B row slot) per stored term,
-    // leaving room for static shared memory
-    int block_cap = (smem_optin - 1024) / 16;
-    int vblock_cap = (smem_optin - 1024) / 12;
-    // largest block-bin item: a row has at most max_row stored terms, an edge fewer
-    long long big = 0;
-    if ((vb.has(BBIG) && max_row > vblock_cap) || (eb.has(BBIG) && max_row > block_cap)) big = max_row;
-    DevBuf<double> d_scratch_k;
-    DevBuf<int2> d_scratch_v;
+    const int exact_cap = (smem_optin - 2048) / 8;
+    const long long max_terms = max_row + 1;       // a row's slots or an edge's pairs, plus the self term
+    const int exact_grid = max_terms > exact_cap ? std::min(32, 2 * sms) : 2 * sms;
+    DevBuf<double> d_scratch;
     long long scratch_stride = 0;
-    if (big > block_cap) {
-        scratch_stride = big;
-        DRESS_TRY(d_scratch_v.alloc((size_t)(2 * sms) * (size_t)big, st));
+    if (max_terms > exact_cap) {
+        scratch_stride = (max_terms + 31) & ~31LL;
+        DRESS_TRY(d_scratch.alloc((size_t)exact_grid * (size_t)scratch_stride, st));
     }
-    DRESS_TRY(set_sweep_attributes<true>(block_cap, vblock_cap));
-    DRESS_TRY(set_sweep_attributes<false>(block_cap, vblock_cap));
+    const size_t exact_smem = (size_t)exact_cap * sizeof(double);
+    DRESS_TRY(set_sweep_attributes<true>(exact_smem));
+    DRESS_TRY(set_sweep_attributes<false>(exact_smem));
 
     DevBuf<unsigned long long> d_maxd;
     DRESS_TRY(d_vd.alloc((size_t)(N > 0 ? N : 1), st));
@@ -642,40 +613,16 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     s.ioff = d_ioff.get(); s.pairs = d_pairs.get();
     s.vd = d_vd.get(); s.maxd = d_maxd.get();
     s.eps = epsilon;
-    s.scratch_k = d_scratch_k.get(); s.scratch_v = d_scratch_v.get(); s.scratch_stride = scratch_stride;
+    s.scratch = d_scratch.get(); s.scratch_stride = scratch_stride; s.exact_cap = exact_cap;
+    s.force_exact = ctx.cfg->exact_sums != 0;
     DevBuf<int> d_qv, d_qe;
     DevBuf<unsigned> d_qcount;
     DRESS_TRY(d_qv.alloc((size_t)(N > 0 ? N : 1), st));
     DRESS_TRY(d_qe.alloc((size_t)(E > 0 ? E : 1), st));
     DRESS_TRY(d_qcount.alloc(2, st));
+    DRESS_CUDA_TRY(cudaMemsetAsync(d_qcount.get(), 0, 2 * sizeof(unsigned), st));
     s.qv = d_qv.get(); s.qe = d_qe.get(); s.qcount = d_qcount.get();
-    s.bkey_v = d_bkey_v.get(); s.bkey_e = d_bkey_e.get();
-    s.bofs_v = d_bofs_v.get(); s.bofs_e = d_bofs_e.get();
-    s.bv0 = vb.start[BBLOCK]; s.be0 = eb.start[BBLOCK];
-    // sorted-term slots of the streamed items (queued ones are sorted into them)
-    DevBuf<double> d_skey, d_tkey;
-    {
-        long long lim[4] = {0, 0, 0, 0};
-        if (vb.has(BMED)) {
-            DRESS_CUDA_TRY(counted_memcpy(&lim[0], d_row_off.get() + vb.start[BMED], sizeof(long long),
-                                           cudaMemcpyDeviceToHost, st));
-            DRESS_CUDA_TRY(counted_memcpy(&lim[1], d_row_off.get() + vb.start[BMED + 1], sizeof(long long),
-                                           cudaMemcpyDeviceToHost, st));
-        }
-        if (eb.has(BMED)) {
-            DRESS_CUDA_TRY(counted_memcpy(&lim[2], d_ioff.get() + eb.start[BMED], sizeof(long long),
-                                           cudaMemcpyDeviceToHost, st));
-            DRESS_CUDA_TRY(counted_memcpy(&lim[3], d_ioff.get() + eb.start[BMED + 1], sizeof(long long),
-                                           cudaMemcpyDeviceToHost, st));
-        }
-        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-        DRESS_TRY(d_skey.alloc((size_t)std::max(1LL, lim[1] - lim[0]), st));
-        DRESS_TRY(d_tkey.alloc((size_t)std::max(1LL, lim[3] - lim[2]), st));
-        s.skey = d_skey.get(); s.sbase = lim[0];
-        s.tkey = d_tkey.get(); s.tbase = lim[2];
-    }
-    LaunchCfg lc{sms, block_cap, vblock_cap, st, ctx.side, ctx.side2, ctx.fork, ctx.join, ctx.join2,
-                 E <= BRANCH_MAX_EDGES ? ctx.side3 : nullptr, ctx.join3};
+    LaunchCfg lc{sms, exact_grid, exact_smem, st, ctx.side, ctx.fork, ctx.join};
     double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + E};
     double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + E};
 

@@ -36,7 +36,10 @@ constexpr int SMALL_MAX_EDGES = 2048;
 // (the per-thread load chains of eight SMs are latency-bound; clusters of 16
 // CTAs measured no better).
 constexpr int CLUSTER_MAX_EDGES = 8192;
-constexpr int SMALL_MAX_DEG = 31;      // rows the register networks take (32 terms with the self term)
+// Rows up to this many neighbours: one thread sums an item's terms, so a
+// longer row would make one thread's serial loop the whole sweep; the
+// multi-kernel fit gives such rows a warp or a block.
+constexpr int SMALL_MAX_DEG = 256;
 
 // The checks of fit_graph's device validation, on the host: rows in order
 // and in range, edge ids and endpoints in range.
@@ -105,8 +108,7 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     L.maxE = E;
     L.maxN = N;
     L.maxk = 1;
-    L.M = 2;                                 // smallest register network that holds a row
-    while (L.M < maxdeg + 1) L.M <<= 1;
+    L.M = maxdeg + 1;
     L.parent_bytes = PL.bytes;
     // On one CTA the graph itself must be staged in shared memory too: read
     // through L2 by a single SM, the sweeps are latency-bound and the
@@ -154,6 +156,7 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     P.kind = ITEM_PLAIN;
     P.k = 0;
     P.fwd = g->variant == DRESS_VARIANT_FORWARD || g->variant == DRESS_VARIANT_BACKWARD;
+    P.force_exact = ctx.cfg->exact_sums != 0;
     P.max_iter = max_iterations;
     P.eps = epsilon;
     P.has_nw = has_nw;
@@ -186,7 +189,7 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     if (one_cta) {
         DRESS_TRY(launch_batch(L, ctx.num_sms, st));
     } else {
-        Status ls = launch_cluster_fit(d_desc.get(), E, N, L.M, lnc, ctx.num_sms, st);
+        Status ls = launch_cluster_fit(d_desc.get(), E, N, lnc, ctx.num_sms, st);
         if (ls.code == DRESSX_EUNSUPPORTED) return Status::Ok();     // the multi-kernel fit takes it
         DRESS_TRY(ls);
     }

@@ -143,11 +143,13 @@ Status plan_request(p_dress_graph_t g, int kind, int k, long long smem_cap, bool
     pl.num_subgraphs = kind == DRESSX_FIT ? 0
                      : k == 0 ? 1 : kind == DRESSX_DELTA ? binom_h(N, k) : perm_h(N, k);
 
-    // batch path: rows of at most 31 neighbours, one fit's state in shared
-    // memory; Delta/Nabla with 1 <= k < N (the other orders are trivial or
-    // in-place fits, served by the lane path)
-    bool batch = maxdeg <= 31 && batch_group_bytes(E, N, pl.k, gsize_for(E)) <= smem_cap - 1024 &&
+    // batch path: one fit's state in shared memory; Delta/Nabla with
+    // 1 <= k < N (the other orders are trivial or in-place fits, served by
+    // the lane path).  A whole-graph fit keeps rows of at most 256
+    // neighbours: one thread sums a row there.
+    bool batch = batch_group_bytes(E, N, pl.k, gsize_for(E)) <= smem_cap - 1024 &&
                  batch_group_bytes(E, N, pl.k, gsize_for(E)) <= BATCH_GROUP_BYTES_MAX;
+    if (kind == DRESSX_FIT) batch = batch && maxdeg <= 256;
     if (kind != DRESSX_FIT) batch = batch && k >= 1 && k < N;
     // a whole-graph fit in the batch kernel runs on one thread group (one
     // SM); above a few thousand edges the single-graph fit, which spreads

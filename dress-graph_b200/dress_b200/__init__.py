@@ -345,12 +345,16 @@ def nabla_fit_many(graphs, k=1, **kw):
     return [r[0] for r in hist_requests(graphs, NABLA, k, **kw)]
 
 
-def configure(device=-1, memory_budget_bytes=0, fit_chunk=0, group_threads=0):
+def configure(device=-1, memory_budget_bytes=0, fit_chunk=0, group_threads=0, exact_sums=0):
+    """Replace the engine configuration (``dressx_configure``).  exact_sums=1
+    sends every sum through the sorted path that backs the certified sums
+    (same bits, slower); tests use it to exercise that path."""
     cfg = _abi.Config()
     cfg.device = int(device)
     cfg.memory_budget_bytes = int(memory_budget_bytes)
     cfg.fit_chunk = int(fit_chunk)
     cfg.group_threads = int(group_threads)
+    cfg.exact_sums = int(exact_sums)
     _check(lib().dressx_configure(ctypes.byref(cfg)))
 
 

@@ -53,7 +53,7 @@ class Config(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int), ("memory_budget_bytes", ctypes.c_size_t),
         ("fit_chunk", ctypes.c_int), ("group_threads", ctypes.c_int),
-        ("reserved", ctypes.c_int * 8),
+        ("exact_sums", ctypes.c_int), ("reserved", ctypes.c_int * 7),
     ]
 
 

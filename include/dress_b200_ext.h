@@ -38,7 +38,10 @@ typedef struct dressx_config_t {
     int     fit_chunk;            /* sweeps launched per convergence check    */
     int     group_threads;        /* threads per subgraph in the batch kernel;
                                      0 = pick from the tuned table            */
-    int     reserved[8];
+    int     exact_sums;           /* 1 = every sum takes the sorted path (the
+                                     fallback of the certified sums; slower,
+                                     same bits); for testing that path        */
+    int     reserved[7];
 } dressx_config_t;
 
 /* Replace the engine configuration; call before the first fit. */

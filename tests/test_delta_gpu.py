@@ -91,15 +91,27 @@ def test_per_fit_path_matches_batched(oracle_port):
     assert a["fits"] == b["fits"] == n
 
 
-def test_wide_rows_use_per_fit_path(oracle_port):
-    """A parent with a 40-neighbour vertex is outside the batched kernel's
-    register networks and runs through the per-subgraph path."""
+def test_wide_rows_are_batched(oracle_port):
+    """Parents with rows of any length run in the batched kernel (the
+    prepared batch refuses requests it cannot batch): a 40-neighbour vertex,
+    and a weighted Chung-Lu parent whose hubs have over 100 neighbours."""
     n = 41
     U = np.array([0] * 40 + list(range(1, 40)), np.int32)
     V = np.array(list(range(1, 41)) + list(range(2, 41)), np.int32)
-    ref = oracle_port.delta_fit(n, U, V, k=1)
-    r = gpu_hist(db.DELTA, n, U, V, k=1)
-    np.testing.assert_array_equal(r["hist"], ref["hist"])
+    cases = [(n, U, V, None)]
+    n2, U2, V2 = graphs.chung_lu(300, 1000, 2.0, 250, seed=3)
+    cases.append((n2, U2, V2, graphs.uniform_weights(len(U2), seed=8)))
+    for n, U, V, W in cases:
+        with db.Graph(n, U, V, W) as g:
+            assert max(np.diff(g.ptr.contents.adj_offset[: n + 1])) >= 40
+            for kind, fn in ((db.DELTA, oracle_port.delta_fit), (db.NABLA, oracle_port.nabla_fit)):
+                b = db.Batch([g], kind, 1)
+                b.run()
+                got = b.fetch()[0]
+                b.close()
+                np.testing.assert_array_equal(got, fn(n, U, V, W, k=1)["hist"])
+    n2, U2, V2, _ = cases[1]
+    assert max(np.bincount(np.concatenate([U2, V2]))) > 100
 
 
 def test_k0_fits_in_place_and_k_ge_n(oracle_port):

@@ -22,11 +22,18 @@ def test_small_graphs_take_the_batch_path():
     assert b_nabla == b_delta
 
 
-def test_hubs_and_trivial_orders_take_a_lane():
-    n, U, V = graphs.chung_lu(2000, 12000, 2.3, 500, seed=2)
+def test_hub_rows():
+    # hub rows: the whole-graph fit runs on the single-graph engine (a warp or
+    # a block per long row); the Delta^1 subgraphs are batched, their rows of
+    # any length summed in the batch kernel
+    n, U, V = graphs.chung_lu(2000, 6000, 2.3, 500, seed=2)
     with db.Graph(n, U, V) as g:
+        assert max(np.diff(g.ptr.contents.adj_offset[: n + 1])) > 256
         assert db.estimate(g, db.FIT)[1] == db.PATH_LANE
-        assert db.estimate(g, db.DELTA, 1)[1] == db.PATH_LANE
+        assert db.estimate(g, db.DELTA, 1)[1] == db.PATH_BATCH
+
+
+def test_trivial_orders_take_a_lane():
     n, U, V = graphs.random_regular(40, 4, seed=3)
     with db.Graph(n, U, V) as g:
         assert db.estimate(g, db.DELTA, 0)[1] == db.PATH_LANE     # k = 0 fits in place
