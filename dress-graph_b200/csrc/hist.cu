@@ -5,11 +5,13 @@
 // ascending by value.  Here every request's converged edge values sit in one
 // contiguous segment of a device buffer; all segments are sorted at once by a
 // segmented LSD radix sort on the order-preserving 64-bit image of the double
-// (8-bit digits, stable in-tile ranking), then run-length encoded.  Runs are
-// cut where neighbouring values differ under ==, so +0.0/-0.0 merge (they are
-// adjacent after the sort) and every NaN is a run of its own, as in the
-// reference's map.  A pass in which every segment has a single digit value
-// moves nothing and is skipped.
+// (8-bit digits, stable in-tile ranking), then run-length encoded.  A run is
+// one bit pattern, as the reference's map keys values by their bits (its
+// hash reads the pattern) and merges them by ==: the only ==-equal values it
+// can keep apart, +0 and -0, hash to different slots and merge only when
+// one's probe run reaches the other; here they are two entries, -0 first.
+// Every NaN is a run of its own (never == itself), as in the map.  A pass in
+// which every segment has a single digit value moves nothing and is skipped.
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
@@ -151,13 +153,13 @@ __global__ void __launch_bounds__(HT) k_tile_scatter(const Tile *tiles, const un
     }
 }
 
-// run heads per tile (segments start a run; == decides equality)
+// run heads per tile: segments start a run, a new bit pattern starts one,
+// and so does every NaN
 __device__ __forceinline__ bool is_head(const unsigned long long *k, long long i, long long seg_begin)
 {
-    if (i == seg_begin) return true;
-    double a = __longlong_as_double((long long)from_ordered(k[i]));
-    double b = __longlong_as_double((long long)from_ordered(k[i - 1]));
-    return !(a == b);
+    if (i == seg_begin || k[i] != k[i - 1]) return true;
+    const double a = __longlong_as_double((long long)from_ordered(k[i]));
+    return a != a;
 }
 
 __global__ void __launch_bounds__(HT) k_tile_heads(const Tile *tiles, const long long *seg_begin,

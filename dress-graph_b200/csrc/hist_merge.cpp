@@ -6,8 +6,9 @@
 // libdress/src/dress_histogram.c:62-81), then flattens it ascending by value
 // (dress_histogram.c:124-155).  Every shard's list here is already sorted and
 // run-length encoded, so one k-way merge over the order-preserving integer
-// image of the values gives the same list: counts of ==-equal values are
-// added, the first value's bits are kept, as in the device histogram.
+// image of the values gives the same list: counts of equal bit patterns are
+// added (the map's key; a NaN never equals an entry and stays apart), as in
+// the device histogram.
 #include <cstdlib>
 #include <cstring>
 #include <queue>
@@ -71,7 +72,7 @@ extern "C" int dressx_hist_merge(const int64_t *const *flats, const int64_t *len
         heap.pop();
         const long long bits = flats[i][pos[(size_t)i]];
         const long long cnt = flats[i][pos[(size_t)i] + 1];
-        if (m > 0 && as_double(res[m - 2]) == as_double(bits)) {
+        if (m > 0 && res[m - 2] == bits && as_double(bits) == as_double(bits)) {
             res[m - 1] += cnt;
         } else {
             res[m] = bits;

@@ -333,17 +333,37 @@ static void vb_push(valbuf_t *b, double x)
     b->v[b->n++] = x;
 }
 
-/* Sorted ascending, runs of ==-equal values merged: the same flat
- * [bits, count, ...] list the reference's hash map flattens to. */
+/* The order-preserving image of a double's bits: ascending by value,
+ * -0 before +0, NaNs at the ends by their bits. */
+static uint64_t ordered_bits(double x)
+{
+    uint64_t u;
+    memcpy(&u, &x, sizeof u);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ULL);
+}
+
+static int cmp_ordered_bits(const void *a, const void *b)
+{
+    uint64_t x = ordered_bits(*(const double *)a), y = ordered_bits(*(const double *)b);
+    return (x > y) - (x < y);
+}
+
+/* The flat [bits, count, ...] list of the reference's hash map
+ * (dress_histogram.c:40-60, 124-155), ascending by value.  The map keys
+ * values by their bits (the hash reads the bit pattern) and merges them by
+ * ==, so the only ==-equal values it can keep apart are +0 and -0: they hash
+ * to different slots and merge only when one's probe run reaches the other.
+ * Here they are two entries, -0 first; a NaN (never == itself) is an entry of
+ * its own each time, as in the map. */
 static int64_t *vb_flatten(valbuf_t *b, int *hist_size)
 {
     if (b->n == 0) { *hist_size = 0; free(b->v); return NULL; }
-    qsort(b->v, b->n, sizeof(double), cmp_double_asc);
+    qsort(b->v, b->n, sizeof(double), cmp_ordered_bits);
     int64_t *out = (int64_t *)malloc(2 * b->n * sizeof(int64_t));
     size_t m = 0, i = 0;
     while (i < b->n) {
         size_t j = i + 1;
-        while (j < b->n && b->v[j] == b->v[i]) ++j;
+        while (j < b->n && b->v[j] == b->v[i] && ordered_bits(b->v[j]) == ordered_bits(b->v[i])) ++j;
         memcpy(&out[2 * m], &b->v[i], sizeof(double));
         out[2 * m + 1] = (int64_t)(j - i);
         ++m; i = j;

@@ -48,6 +48,23 @@ TOPOLOGIES = {
 }
 
 
+def long_parallel_runs():
+    """Multigraphs whose rows hold long runs of parallel edges to one
+    neighbour.  The reference sorts each row by neighbour id only
+    (libdress/src/dress.c:25-30, 283-293) with the C library's qsort, so the
+    order inside such a run -- which decides how the merge walk pairs
+    parallel edges -- is the qsort's; these cases pin it (the C library the
+    fixtures were made with is recorded in golden_meta.json)."""
+    rng = np.random.default_rng(31)
+    U = [0] * 40 + [1] * 25 + [0, 0, 1, 2, 3, 4] + [2] * 12
+    V = [1] * 40 + [2] * 25 + [2, 3, 3, 3, 4, 0] + [4] * 12
+    order = rng.permutation(len(U))                 # parallel edges listed out of order
+    U = [U[i] for i in order]
+    V = [V[i] for i in order]
+    W = rng.uniform(0.5, 2.0, len(U)).round(6).tolist()
+    return {"multi_long_runs": (5, U, V, None), "multi_long_runs_w": (5, U, V, W)}
+
+
 def bits(a):
     return np.asarray(a, dtype=np.float64).view(np.int64).tolist()
 
@@ -70,6 +87,7 @@ def main():
         raise SystemExit("build the reference first: make -C oracle ref")
     cases = dict(TOPOLOGIES)
     cases.update(random_cases())
+    cases.update(long_parallel_runs())
     fits, hists = [], []
     for name, (n, U, V, W) in cases.items():
         for variant in range(4):
@@ -99,6 +117,11 @@ def main():
         json.dump(fits, f)
     with gzip.open(os.path.join(HERE, "hist_cases.json.gz"), "wt") as f:
         json.dump(hists, f)
+    import platform
+    with open(os.path.join(HERE, "golden_meta.json"), "w") as f:
+        json.dump({"made_by": "the reference library compiled unchanged (oracle/_ref/libdress_ref.so)",
+                   "libc": " ".join(platform.libc_ver()), "fit_cases": len(fits), "hist_cases": len(hists)},
+                  f, indent=1)
     print(len(fits), "fit cases,", len(hists), "histogram cases")
 
 

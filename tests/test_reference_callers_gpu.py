@@ -34,10 +34,13 @@ def test_reference_cuda_test_binary():
     if not os.path.exists(exe):
         pytest.skip("reference CUDA test not built")
     # The test's graph copies leave NW and max_degree uninitialised
-    # (tests/c/cuda/test_dress_cuda.c:25-86) and its dress_free_graph frees
-    # NW; MALLOC_PERTURB_=255 makes glibc hand out zero-filled memory, i.e.
-    # the NULL vertex weights (all 1.0) the test means.
-    env = dict(os.environ, MALLOC_PERTURB_="255")
+    # (tests/c/cuda/test_dress_cuda.c:25-86) and the reference's
+    # dress_free_graph frees NW (libdress/src/dress.c:630): with stale heap
+    # contents the binary aborts in malloc even when dress_fit_cuda does
+    # nothing.  MALLOC_PERTURB_=255 makes glibc fill new allocations with
+    # zeros, and the tcache (whose fast path skips that fill) is turned off,
+    # so NW reads as NULL -- the unit vertex weights the test means.
+    env = dict(os.environ, MALLOC_PERTURB_="255", GLIBC_TUNABLES="glibc.malloc.tcache_count=0")
     out = subprocess.run([exe], capture_output=True, text=True, timeout=600, env=env)
     text = out.stdout + out.stderr
     assert out.returncode == 0, text[-4000:]

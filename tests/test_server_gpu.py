@@ -36,7 +36,8 @@ def rr_graph(rng, e_target):
 
 def make_mix(seed=11):
     """(kind, n, U, V, W) tuples: 36 small fits, 3 large fits, 8 Delta^1,
-    2 Nabla^1, 2 hub Delta^1 (lane path)."""
+    2 Nabla^1, 2 hub Delta^1 (batched: rows of any length) and one dense
+    Delta^1 whose subgraph state exceeds shared memory (lane path)."""
     rng = np.random.default_rng(seed)
     mix = []
     for _ in range(36):
@@ -56,6 +57,8 @@ def make_mix(seed=11):
     for m in (300, 500):
         n, U, V = graphs.chung_lu(60, m, 2.3, 50, seed=int(rng.integers(1 << 30)))
         mix.append((db.DELTA, n, U, V, graphs.uniform_weights(len(U), seed=5)))
+    n, U, V = graphs.erdos_renyi(200, 15000, seed=int(rng.integers(1 << 30)))
+    mix.append((db.DELTA, n, U, V, None))
     order = rng.permutation(len(mix))
     return [mix[i] for i in order]
 

@@ -84,3 +84,16 @@ def test_two_gloo_ranks_gather_and_merge():
     expect = flat_of(np.concatenate(rng_vals))
     for o in outs:                       # every rank holds the same merged histogram
         np.testing.assert_array_equal(o, expect)
+
+
+def test_merge_keys_by_bits():
+    """Equal bit patterns merge; +0 and -0 stay two entries (-0 first), and
+    every NaN is an entry of its own, as in the reference's map."""
+    pz, nz = np.float64(0.0).view(np.int64), np.float64(-0.0).view(np.int64)
+    nan = np.float64(np.nan).view(np.int64)
+    a = np.array([nz, 2, pz, 3], np.int64)
+    b = np.array([nz, 1, pz, 4, nan, 1], np.int64)
+    got = shard.merge_hists([a, b])
+    np.testing.assert_array_equal(got, np.array([nz, 3, pz, 7, nan, 1], np.int64))
+    got = shard.merge_hists([b, b])
+    np.testing.assert_array_equal(got, np.array([nz, 2, pz, 8, nan, 1, nan, 1], np.int64))
