@@ -713,15 +713,25 @@ std::mutex g_na_mu;
 unsigned char *g_na_base[NA_MAX_DEVICES];      // device address of the array, per device
 
 // The array's name is a host-side stand-in in host code; its device address
-// comes from cudaGetSymbolAddress, once per device, with that device current.
-cudaError_t noalloc_scratch(unsigned char **out)
+// comes from cudaGetSymbolAddress with the device current.  Outside stream
+// capture every call looks it up afresh (a cudaDeviceReset or another
+// context made current then cannot leave a stale address behind); while
+// `st` is being captured the address of the device's last call outside
+// capture is used, so the first call on a device must come before any
+// capture.
+cudaError_t noalloc_scratch(cudaStream_t st, unsigned char **out)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= NA_MAX_DEVICES) return cudaErrorInvalidDevice;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        cs = cudaStreamCaptureStatusActive;
+    }
     std::lock_guard<std::mutex> lk(g_na_mu);
-    if (!g_na_base[dev]) {
+    if (cs == cudaStreamCaptureStatusNone || !g_na_base[dev]) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
@@ -749,7 +759,7 @@ extern "C" int dressx_histogram_noalloc(const double *values, int64_t n, int64_t
     }
     cudaStream_t st = (cudaStream_t)stream;
     unsigned char *base = nullptr;
-    cudaError_t e = noalloc_scratch(&base);
+    cudaError_t e = noalloc_scratch(st, &base);
     if (e != cudaSuccess) {
         std::fprintf(stderr, "dress_b200: dressx_histogram_noalloc: scratch address: %s\n", cudaGetErrorString(e));
         return DRESSX_ECUDA;

@@ -155,13 +155,16 @@ int dressx_counters(int64_t *h2d_bytes, int64_t *d2h_bytes, int64_t *launches, i
  *   values   device pointer, n doubles (n <= DRESSX_NOALLOC_MAX_VALUES;
  *            larger n returns DRESSX_EUNSUPPORTED and enqueues nothing)
  *   pairs    device pointer, room for 2*n int64: [value bits, count, ...]
- *            ascending by value, ==-equal values merged as in
- *            dressx_hist_batch
+ *            ascending by value, one entry per bit pattern (+0 and -0
+ *            apart, every NaN apart) as in dressx_hist_batch
  *   num_runs device pointer, one int64: the number of (value, count) pairs
  *   stream   cudaStream_t the work is enqueued on (NULL = legacy stream)
  * Nothing is synchronised: results are valid once the stream has run the
- * enqueued work.  The first call on a device looks up the array's device
- * address; make that first call before any stream capture starts.  Every
+ * enqueued work.  A call made outside stream capture looks up the array's
+ * device address in the current context (so a device reset or a switch of
+ * context is followed); a call on a stream under capture reuses the address
+ * of the device's last call outside capture, so make the first call on a
+ * device before any stream capture starts.  Every
  * call uses the same array, so calls whose work overlaps on the GPU (other
  * streams, other host threads) race and must be serialised by the caller. */
 #define DRESSX_NOALLOC_MAX_VALUES (1 << 20)
@@ -192,7 +195,7 @@ int dressx_get_batch(p_dress_graph_t g, const int *u, const int *v, int64_t n, i
  * strided slices offset = rank, stride = ranks of several GPUs or
  * processes): n flat [value_bits, count, ...] lists, each ascending by value,
  * into one list of the same form (malloc'd; *out_len entries).  Counts of
- * ==-equal values add up.  Replaces the gather-and-reinsert step of the
+ * equal bit patterns add up (a NaN stays an entry of its own).  Replaces the gather-and-reinsert step of the
  * reference's MPI layer (libdress/src/mpi/dress_mpi.c:90-118). */
 int dressx_hist_merge(const int64_t *const *flats, const int64_t *lens, int n, int64_t **out,
                       int64_t *out_len);
