@@ -31,3 +31,48 @@ def test_strided_shards_match_oracle(oracle_port):
         ref = oracle_port.delta_fit(n, U, V, k=1, offset=r, stride=3)["hist"]
         np.testing.assert_array_equal(parts[r], ref)
     np.testing.assert_array_equal(shard.merge_hists(parts), oracle_port.delta_fit(n, U, V, k=1)["hist"])
+
+
+def _fit_rank(rank, world, port, path, kind, k):
+    """One rank of shard.fit_sharded: its stride on cuda:0 through the
+    engine, the histograms all-gathered over gloo and merged."""
+    import os
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        torch.cuda.set_device(0)
+        n, U, V = graphs.random_regular(36, 6, seed=12)
+        with db.Graph(n, U, V) as g:
+            merged, nsub, fits = shard.fit_sharded(g, kind, k)
+        np.save(f"{path}.{rank}.npy", np.concatenate([[nsub, fits], merged]).astype(np.int64))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("kind,k", [(db.DELTA, 1), (db.NABLA, 1)])
+def test_fit_sharded_two_ranks(oracle_port, kind, k):
+    """shard.fit_sharded end to end: two processes (gloo ranks) each run
+    their stride through the engine on the same GPU (no kernel of one waits
+    on the other), all-gather and merge; every rank's merged histogram is
+    the oracle's unsharded one."""
+    import os
+    import socket
+    import tempfile
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    world = 2
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "h")
+        mp.spawn(_fit_rank, args=(world, port, path, kind, k), nprocs=world, join=True)
+        outs = [np.load(f"{path}.{r}.npy") for r in range(world)]
+    n, U, V = graphs.random_regular(36, 6, seed=12)
+    fn = oracle_port.delta_fit if kind == db.DELTA else oracle_port.nabla_fit
+    ref = fn(n, U, V, k=k)
+    for o in outs:
+        assert o[0] == ref["num"]
+        assert o[1] == ref["num"]                  # every subgraph of a regular graph has edges
+        np.testing.assert_array_equal(o[2:], ref["hist"])
