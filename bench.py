@@ -413,7 +413,7 @@ def bench_single_fit(args, torch):
             "iterations": it, "sweeps": sweeps, "delta": dl, "common_terms": st["common_terms"],
             "edge_iters_per_s": E * sweeps / (st["iterate_ms"] / 1e3),
             "edge_iters_per_s_e2e": E * sweeps / wall,
-            "sweep_ms": sweep_ms, "setup_ms": st["setup_ms"], "e2e_ms": wall * 1e3,
+            "sweep_ms": sweep_ms, "setup_ms": st["setup_ms"], "e2e_ms": wall * 1e3, "phases_ms": st["phases_ms"],
             "h2d_bytes": cnt["h2d_bytes"], "d2h_bytes": cnt["d2h_bytes"], "launches": cnt["launches"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,

@@ -12,6 +12,7 @@
 #include <algorithm>
 
 #include "engine.h"
+#include "host_par.h"
 
 namespace dress {
 
@@ -59,6 +60,104 @@ Status Pinned::reserve(size_t bytes)
     cap_ = bytes;
     return Status::Ok();
 }
+
+// ---- staged copies ----------------------------------------------------------
+namespace {
+
+// Pieces of the byte range [lo, hi) of the spans taken as one range, in span
+// order: fn(span, offset in the span, length, offset from lo).
+template <class F>
+void for_pieces(const HostSpan *spans, int n, size_t lo, size_t hi, F fn)
+{
+    size_t base = 0;
+    for (int i = 0; i < n && base < hi; ++i) {
+        const size_t b = std::max(lo, base), e = std::min(hi, base + spans[i].bytes);
+        if (b < e) fn(spans[i], b - base, e - b, b - lo);
+        base += spans[i].bytes;
+    }
+}
+
+// host memcpy of chunk k between its stage slot and the spans, split over
+// host threads in 4 MiB grains
+void host_part(const HostSpan *spans, int n, char *stage, size_t k, size_t total, bool to_stage)
+{
+    constexpr size_t grain = (size_t)4 << 20;
+    char *slot = stage + (k & 1) * STAGE_CHUNK;
+    const size_t lo = k * STAGE_CHUNK, hi = std::min(total, lo + STAGE_CHUNK);
+    const long long pieces = (long long)((hi - lo + grain - 1) / grain);
+    parallel_for(pieces, host_threads(pieces), [&](long long g) {
+        const size_t a = lo + (size_t)g * grain, b = std::min(hi, a + grain);
+        for_pieces(spans, n, a, b, [&](const HostSpan &sp, size_t off, size_t len, size_t at) {
+            char *st = slot + (a - lo) + at;
+            if (to_stage) std::memcpy(st, (const char *)sp.host + off, len);
+            else std::memcpy((char *)sp.host + off, st, len);
+        });
+    });
+}
+
+Status staged_copy(const HostSpan *spans, int n, const Ctx &ctx, bool up)
+{
+    size_t total = 0;
+    for (int i = 0; i < n; ++i) total += spans[i].bytes;
+    if (total == 0) return Status::Ok();
+    if (total <= ((size_t)1 << 20) || !ctx.stage) {
+        // small copies: the driver's own staging is as quick
+        for (int i = 0; i < n; ++i) {
+            if (!spans[i].bytes) continue;
+            if (up) DRESS_CUDA_TRY(counted_memcpy(spans[i].dev, spans[i].host, spans[i].bytes, cudaMemcpyHostToDevice, ctx.st));
+            else DRESS_CUDA_TRY(counted_memcpy(spans[i].host, spans[i].dev, spans[i].bytes, cudaMemcpyDeviceToHost, ctx.st));
+        }
+        DRESS_CUDA_TRY(cudaStreamSynchronize(ctx.st));
+        return Status::Ok();
+    }
+    DRESS_TRY(ctx.stage->reserve(2 * STAGE_CHUNK));
+    char *stage = ctx.stage->ptr();
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    for (auto &e : ev) DRESS_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    struct EvGuard {
+        cudaEvent_t *e;
+        ~EvGuard()
+        {
+            cudaEventSynchronize(e[0]);
+            cudaEventSynchronize(e[1]);
+            cudaEventDestroy(e[0]);
+            cudaEventDestroy(e[1]);
+        }
+    } guard{ev};
+    const size_t nchunks = (total + STAGE_CHUNK - 1) / STAGE_CHUNK;
+    for (size_t k = 0; k < nchunks; ++k) {
+        char *slot = stage + (k & 1) * STAGE_CHUNK;
+        const size_t lo = k * STAGE_CHUNK, hi = std::min(total, lo + STAGE_CHUNK);
+        if (k >= 2) DRESS_CUDA_TRY(cudaEventSynchronize(ev[k & 1]));     // the slot's last copy is done
+        if (up) host_part(spans, n, stage, k, total, true);
+        Status err;
+        for_pieces(spans, n, lo, hi, [&](const HostSpan &sp, size_t off, size_t len, size_t at) {
+            cudaError_t e = up ? cudaMemcpyAsync((char *)sp.dev + off, slot + at, len, cudaMemcpyHostToDevice, ctx.st)
+                               : cudaMemcpyAsync(slot + at, (const char *)sp.dev + off, len, cudaMemcpyDeviceToHost,
+                                                 ctx.st);
+            if (e != cudaSuccess && err.ok()) err = Status::Err(DRESSX_ECUDA, cudaGetErrorString(e));
+        });
+        DRESS_TRY(err);
+        if (up) count_h2d(hi - lo);
+        else count_d2h(hi - lo);
+        DRESS_CUDA_TRY(cudaEventRecord(ev[k & 1], ctx.st));
+        if (!up && k >= 1) {
+            // the previous chunk is on the host: copy it out while this one is in flight
+            DRESS_CUDA_TRY(cudaEventSynchronize(ev[(k - 1) & 1]));
+            host_part(spans, n, stage, k - 1, total, false);
+        }
+    }
+    if (!up) {
+        DRESS_CUDA_TRY(cudaEventSynchronize(ev[(nchunks - 1) & 1]));
+        host_part(spans, n, stage, nchunks - 1, total, false);
+    }
+    return Status::Ok();
+}
+
+}  // namespace
+
+Status staged_upload(const HostSpan *spans, int n, const Ctx &ctx) { return staged_copy(spans, n, ctx, true); }
+Status staged_download(const HostSpan *spans, int n, const Ctx &ctx) { return staged_copy(spans, n, ctx, false); }
 
 thread_local cudaMemPool_t tls_pool = nullptr;
 thread_local long long tls_launches = 0;
@@ -183,6 +282,7 @@ int dressx_last_fit_stats(dressx_fit_stats_t *out)
         out->edge_bin_items[b] = g_last_stats.ebin_items[b];
         out->edge_bin_terms[b] = g_last_stats.ebin_terms[b];
     }
+    for (int i = 0; i < 5; ++i) out->phase_ms[i] = g_last_stats.phase_ms[i];
     return DRESSX_OK;
 }
 

@@ -147,6 +147,21 @@ inline cudaError_t counted_memcpy(void *dst, const void *src, size_t n, cudaMemc
     return cudaMemcpyAsync(dst, src, n, kind, st);
 }
 
+// ---- staged copies between pageable host memory and the device -------------
+// A pageable cudaMemcpy moves through the driver's own small staging at a
+// fraction of the link's speed.  These copy a list of spans through the
+// context's pinned stage instead, in chunks of STAGE_CHUNK bytes: host
+// threads fill one half of the stage while the copy engine drains the other.
+// Both return once every copy has completed (the stage is free again).
+struct HostSpan {
+    void *host;
+    void *dev;
+    size_t bytes;
+};
+constexpr size_t STAGE_CHUNK = (size_t)32 << 20;
+Status staged_upload(const HostSpan *spans, int n, const Ctx &ctx);
+Status staged_download(const HostSpan *spans, int n, const Ctx &ctx);
+
 // ---- device utilities (scan.cu) -------------------------------------------
 // out[i] = sum_{j<i} in[i] for i in [0, n], out[n] = total.  `tmp` must hold
 // scan_tmp_elems(n) int64 values.
@@ -159,6 +174,9 @@ struct FitStats {
     long long T = 0;            // common-neighbour terms per sweep
     int sweeps = 0;             // sweeps executed
     double setup_ms = 0, iterate_ms = 0;
+    // host time of the fit's phases: upload, validation, common-neighbour
+    // tables and bins, renumbering and sweep set-up, results download
+    double phase_ms[5] = {};
     long long vbin_items[8] = {}, vbin_terms[8] = {}, ebin_items[8] = {}, ebin_terms[8] = {};
 };
 Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon,

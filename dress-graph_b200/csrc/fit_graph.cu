@@ -32,12 +32,14 @@
 
 #include "common.cuh"
 #include "engine.h"
+#include "hist.h"
 #include "sweep.cuh"
 
 namespace dress {
 namespace {
 
 constexpr int MAX_CHUNK = 32;      // sweeps launched per host check (<= RING/2)
+constexpr int LOCALITY_MIN_EDGES = 1 << 20;   // graphs renumbered for gather locality
 using namespace sweep;
 
 __device__ __forceinline__ unsigned lanemask_lt()
@@ -252,6 +254,63 @@ __global__ void k_bin_scatter(int n, const int *len, int *cursor, int *perm, int
     }
 }
 
+// Sort keys of the edge renumbering.  Fine bin first (so every bin is one
+// contiguous range); block bins then largest first (the longest sums start
+// first); thread and warp bins by owner -- the endpoint of lower (degree, id)
+// rank, the triangle listing's orientation -- in the new vertex numbering,
+// then by the other endpoint.  A vertex owns most edges of its row unless it
+// is a hub, so its row's edges, and the (u, x) edges of the common-neighbour
+// pairs of its edges, sit next to each other: neighbouring lanes gather
+// neighbouring products.
+__global__ void k_edge_keys(int E, int N, const int *U, const int *V, const int *deg, const int *vinv,
+                            const int *cnt, unsigned long long *keys, unsigned *vals)
+{
+    const bool wide = N > (1 << 27);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const int c = cnt[e];
+        const unsigned long long f = (unsigned long long)fine_of((long long)c);
+        unsigned long long low;
+        if (bin_of((long long)c) >= BBLOCK) {
+            low = (1ULL << 54) - 1 - (unsigned long long)c;
+        } else {
+            const int u = U[e], v = V[e];
+            const bool uo = rank_key(deg, u) <= rank_key(deg, v);
+            const unsigned long long o = (unsigned)vinv[uo ? u : v], x = (unsigned)vinv[uo ? v : u];
+            low = wide ? o : (o << 27) | x;
+        }
+        keys[e] = (f << 54) | low;
+        vals[e] = (unsigned)e;
+    }
+}
+
+__global__ void k_inverse(int n, const unsigned *perm, int *pinv, int *inv)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        pinv[i] = (int)perm[i];
+        inv[perm[i]] = i;
+    }
+}
+
+// pairs of each edge keyed (edge, e_ux): a sort groups them by edge (in
+// order, so the offsets stay) and orders each edge's pairs by e_ux
+__global__ void k_pair_keys(int E, const long long *ioff, const int2 *pairs, unsigned long long *keys, unsigned *vals)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
+        const long long b = ioff[j], n = ioff[j + 1] - b;
+        for (long long k = 0; k < n; ++k) {
+            const int2 pr = pairs[b + k];
+            keys[b + k] = ((unsigned long long)(unsigned)j << 32) | (unsigned)pr.x;
+            vals[b + k] = (unsigned)pr.y;
+        }
+    }
+}
+
+__global__ void k_pairs_from_keys(long long T, const unsigned long long *keys, const unsigned *vals, int2 *pairs)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < T; i += (long long)gridDim.x * blockDim.x)
+        pairs[i] = make_int2((int)(unsigned)(keys[i] & 0xffffffffULL), (int)vals[i]);
+}
+
 __global__ void k_gather_seg(int n, const int *perm, const int *len, int *out)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = len[perm[i]];
@@ -322,14 +381,6 @@ __global__ void k_unpermute(int n, const int *perm, const double *src, double *d
         dst[perm[i]] = src[i];
 }
 
-template <class T>
-Status upload(DevBuf<T> &b, const T *host, size_t n, cudaStream_t st)
-{
-    DRESS_TRY(b.alloc(n, st));
-    if (n) DRESS_CUDA_TRY(counted_memcpy(b.get(), host, n * sizeof(T), cudaMemcpyHostToDevice, st));
-    return Status::Ok();
-}
-
 double ms_since(std::chrono::steady_clock::time_point t0)
 {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -366,22 +417,32 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     const int sms = ctx.num_sms;
     const int fwd = (g->variant == DRESS_VARIANT_FORWARD || g->variant == DRESS_VARIANT_BACKWARD);
 
-    // ---- upload --------------------------------------------------------
+    // ---- upload: every array through the pinned stage in one pipeline ------
     DevBuf<int> d_off, d_tgt, d_eidx, d_U, d_V;
     DevBuf<double> d_w, d_d, d_nw;
-    DRESS_TRY(upload(d_off, g->adj_offset, (size_t)N + 1, st));
-    DRESS_TRY(upload(d_tgt, g->adj_target, (size_t)S, st));
-    DRESS_TRY(upload(d_eidx, g->adj_edge_idx, (size_t)S, st));
-    DRESS_TRY(upload(d_U, g->U, (size_t)E, st));
-    DRESS_TRY(upload(d_V, g->V, (size_t)E, st));
-    DRESS_TRY(upload(d_w, g->edge_weight, (size_t)E, st));
-    DRESS_TRY(upload(d_d, g->edge_dress, (size_t)E, st));
-    if (g->NW) {
-        DRESS_TRY(upload(d_nw, g->NW, (size_t)N, st));
-    } else {                                   // NULL vertex weights mean all 1.0
-        DRESS_TRY(d_nw.alloc((size_t)N, st));
-        if (N) count_launch(), k_fill<<<grid_for(N, 256, 16 * sms), 256, 0, st>>>(N, 1.0, d_nw.get());
+    DRESS_TRY(d_off.alloc((size_t)N + 1, st));
+    DRESS_TRY(d_tgt.alloc((size_t)S, st));
+    DRESS_TRY(d_eidx.alloc((size_t)S, st));
+    DRESS_TRY(d_U.alloc((size_t)E, st));
+    DRESS_TRY(d_V.alloc((size_t)E, st));
+    DRESS_TRY(d_w.alloc((size_t)E, st));
+    DRESS_TRY(d_d.alloc((size_t)E, st));
+    DRESS_TRY(d_nw.alloc((size_t)N, st));
+    {
+        std::vector<HostSpan> spans = {
+            {g->adj_offset, d_off.get(), ((size_t)N + 1) * sizeof(int)},
+            {g->adj_target, d_tgt.get(), (size_t)S * sizeof(int)},
+            {g->adj_edge_idx, d_eidx.get(), (size_t)S * sizeof(int)},
+            {g->U, d_U.get(), (size_t)E * sizeof(int)},
+            {g->V, d_V.get(), (size_t)E * sizeof(int)},
+            {g->edge_weight, d_w.get(), (size_t)E * sizeof(double)},
+            {g->edge_dress, d_d.get(), (size_t)E * sizeof(double)}};
+        if (g->NW) spans.push_back({g->NW, d_nw.get(), (size_t)N * sizeof(double)});
+        DRESS_TRY(staged_upload(spans.data(), (int)spans.size(), ctx));
     }
+    const double t_upload = ms_since(t0);
+    if (!g->NW && N)                           // NULL vertex weights mean all 1.0
+        count_launch(), k_fill<<<grid_for(N, 256, 16 * sms), 256, 0, st>>>(N, 1.0, d_nw.get());
 
     // ---- validate ----------------------------------------------------------
     DevBuf<int> d_flags, d_deg, d_cnt;
@@ -397,6 +458,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     int flags[8];
     DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    const double t_validate = ms_since(t0);
     if (flags[0]) return Status::Err(DRESSX_EINVAL, "malformed graph (CSR or edge endpoints out of range)");
     const bool dup = flags[1] != 0;
     const bool uniform = flags[2] == 0;
@@ -412,11 +474,15 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     const int eg = (int)grid_for(E, 256, 32 * sms);
     if (g->precompute_intercepts && g->intercept_offset) {
         DevBuf<int> d_io, d_ux, d_vx;
-        DRESS_TRY(upload(d_io, g->intercept_offset, (size_t)E + 1, st));
         long long Tg = g->intercept_offset[E];
         if (Tg < 0) return Status::Err(DRESSX_EINVAL, "bad intercept_offset");
-        DRESS_TRY(upload(d_ux, g->intercept_edge_ux, (size_t)Tg, st));
-        DRESS_TRY(upload(d_vx, g->intercept_edge_vx, (size_t)Tg, st));
+        DRESS_TRY(d_io.alloc((size_t)E + 1, st));
+        DRESS_TRY(d_ux.alloc((size_t)Tg, st));
+        DRESS_TRY(d_vx.alloc((size_t)Tg, st));
+        const HostSpan spans[3] = {{g->intercept_offset, d_io.get(), ((size_t)E + 1) * sizeof(int)},
+                                   {g->intercept_edge_ux, d_ux.get(), (size_t)Tg * sizeof(int)},
+                                   {g->intercept_edge_vx, d_vx.get(), (size_t)Tg * sizeof(int)}};
+        DRESS_TRY(staged_upload(spans, 3, ctx));
         count_launch(), k_given_counts<<<eg, 256, 0, st>>>(E, d_io.get(), d_cnt.get(), d_flags.get());
         DRESS_TRY(exclusive_scan_i32(d_cnt.get(), d_ioff_old.get(), E, d_scan_tmp.get(), st));
         DRESS_CUDA_TRY(counted_memcpy(&T, d_ioff_old.get() + E, sizeof(T), cudaMemcpyDeviceToHost, st));
@@ -489,6 +555,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_CUDA_TRY(counted_memcpy(bc.data(), d_bc.get(), 2 * NF * sizeof(int), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    const double t_pairs = ms_since(t0);
     if (flags[0]) return Status::Err(DRESSX_EINVAL, "malformed intercept tables");
     // fine ranges (cursors), then the coarse bins they make up
     std::vector<int> cur(2 * NF);
@@ -507,14 +574,35 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     eb.start[NB] = E;
     DRESS_CUDA_TRY(counted_memcpy(d_bc.get() + 2 * NF, cur.data(), 2 * NF * sizeof(int), cudaMemcpyHostToDevice, st));
     count_launch(), k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), d_bc.get() + 2 * NF, d_vperm.get(), d_vinv.get());
-    count_launch(), k_bin_scatter<<<eg, 256, 0, st>>>(E, d_cnt.get(), d_bc.get() + 3 * NF, d_eperm.get(), d_einv.get());
-    // block items largest first, so the longest sequential sums start first
+    // Edges of a large graph: one stable radix sort on (fine bin, owner,
+    // other endpoint), for the locality of the sweeps' gathers.  A small
+    // graph's sweeps are bound by launch latency and its arrays sit in L2, so
+    // it keeps the one-pass scatter (the sort's passes cost more than they save).
+    const bool locality = E >= LOCALITY_MIN_EDGES;
+    if (!locality)
+        count_launch(), k_bin_scatter<<<eg, 256, 0, st>>>(E, d_cnt.get(), d_bc.get() + 3 * NF, d_eperm.get(), d_einv.get());
+    if (locality) {
+        DevBuf<unsigned long long> k0, k1;
+        DevBuf<unsigned> v0, v1;
+        DRESS_TRY(k0.alloc((size_t)E, st));
+        DRESS_TRY(k1.alloc((size_t)E, st));
+        DRESS_TRY(v0.alloc((size_t)E, st));
+        DRESS_TRY(v1.alloc((size_t)E, st));
+        count_launch(), k_edge_keys<<<eg, 256, 0, st>>>(E, N, d_U.get(), d_V.get(), d_deg.get(), d_vinv.get(),
+                                                        d_cnt.get(), k0.get(), v0.get());
+        unsigned long long *sk = nullptr;
+        unsigned *sv = nullptr;
+        DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), E, &sk, &sv, st, sms));
+        count_launch(), k_inverse<<<eg, 256, 0, st>>>(E, sv, d_eperm.get(), d_einv.get());
+    }
+    // block items largest first, so the longest sums start first (the sort
+    // above already ordered the edges of a large graph)
     {
         struct Seg { int *perm, *inv; const int *len; int b0, b1; };
         Seg segs[4] = {{d_vperm.get(), d_vinv.get(), d_deg.get(), vb.start[BBLOCK], vb.start[BBLOCK + 1]},
                        {d_vperm.get(), d_vinv.get(), d_deg.get(), vb.start[BBIG], vb.start[BBIG + 1]},
-                       {d_eperm.get(), d_einv.get(), d_cnt.get(), eb.start[BBLOCK], eb.start[BBLOCK + 1]},
-                       {d_eperm.get(), d_einv.get(), d_cnt.get(), eb.start[BBIG], eb.start[BBIG + 1]}};
+                       {d_eperm.get(), d_einv.get(), d_cnt.get(), locality ? 0 : eb.start[BBLOCK], locality ? 0 : eb.start[BBLOCK + 1]},
+                       {d_eperm.get(), d_einv.get(), d_cnt.get(), locality ? 0 : eb.start[BBIG], locality ? 0 : eb.start[BBIG + 1]}};
         for (const Seg &g2 : segs) {
             const int n = g2.b1 - g2.b0;
             if (n < 2) continue;
@@ -569,8 +657,25 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     count_launch(), k_new_pairs<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_ioff_old.get(), d_pairs_old.get(), d_einv.get(),
                                     d_ioff.get(), d_pairs.get());
     DRESS_CUDA_TRY(cudaGetLastError());
+    d_pairs_old.release();
+    // each edge's pairs in e_ux order: a warp's lanes then gather neighbouring
+    // products (an owner's edges are contiguous)
+    if (locality && T > 1) {
+        DevBuf<unsigned long long> k0, k1;
+        DevBuf<unsigned> v0, v1;
+        DRESS_TRY(k0.alloc((size_t)T, st));
+        DRESS_TRY(k1.alloc((size_t)T, st));
+        DRESS_TRY(v0.alloc((size_t)T, st));
+        DRESS_TRY(v1.alloc((size_t)T, st));
+        count_launch(), k_pair_keys<<<eg, 256, 0, st>>>(E, d_ioff.get(), d_pairs.get(), k0.get(), v0.get());
+        unsigned long long *sk = nullptr;
+        unsigned *sv = nullptr;
+        DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), T, &sk, &sv, st, sms));
+        count_launch(), k_pairs_from_keys<<<grid_for(T, 256, 64 * sms), 256, 0, st>>>(T, sk, sv, d_pairs.get());
+        DRESS_CUDA_TRY(cudaGetLastError());
+    }
     d_U.release(); d_V.release(); d_w.release(); d_d.release(); d_nw.release();
-    d_pairs_old.release(); d_ioff_old.release(); d_ncnt.release(); d_cnt.release(); d_deg.release();
+    d_ioff_old.release(); d_ncnt.release(); d_cnt.release(); d_deg.release();
 
     // exact sums of queued items: shared memory for their terms, a global
     // scratch slice per block for items beyond it
@@ -726,15 +831,14 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     // ---- results back in the caller's numbering ------------------------------
     DevBuf<double> d_out;
     DRESS_TRY(d_out.alloc((size_t)E + N + 1, st));
+    const auto t_down0 = std::chrono::steady_clock::now();
     count_launch(), k_unpermute<<<eg, 256, 0, st>>>(E, d_eperm.get(), dbuf[(last + 1) & 1], d_out.get());
     count_launch(), k_unpermute<<<vg, 256, 0, st>>>(N, d_vperm.get(), d_vd.get(), d_out.get() + E);
-    if (E > 0)
-        DRESS_CUDA_TRY(counted_memcpy(g->edge_dress, d_out.get(), (size_t)E * sizeof(double),
-                                       cudaMemcpyDeviceToHost, st));
-    if (N > 0)
-        DRESS_CUDA_TRY(counted_memcpy(g->vertex_dress, d_out.get() + E, (size_t)N * sizeof(double),
-                                       cudaMemcpyDeviceToHost, st));
-    DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    {
+        const HostSpan spans[2] = {{g->edge_dress, d_out.get(), (size_t)E * sizeof(double)},
+                                   {g->vertex_dress, d_out.get() + E, (size_t)N * sizeof(double)}};
+        DRESS_TRY(staged_download(spans, 2, ctx));
+    }
     if (iterations) *iterations = conv >= 0 ? conv : max_iterations;
     if (delta) *delta = last_delta;
     if (stats) {
@@ -748,6 +852,11 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         stats->sweeps = last + 1;
         stats->setup_ms = setup_ms;
         stats->iterate_ms = sweep_ms;
+        stats->phase_ms[0] = t_upload;
+        stats->phase_ms[1] = t_validate - t_upload;
+        stats->phase_ms[2] = t_pairs - t_validate;
+        stats->phase_ms[3] = setup_ms - t_pairs;
+        stats->phase_ms[4] = ms_since(t_down0);
     }
     return Status::Ok();
 }

@@ -69,7 +69,8 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     used = false;
     const auto t0 = std::chrono::steady_clock::now();
     const int N = g->N, E = g->E;
-    if (E < 1 || E > CLUSTER_MAX_EDGES || N < 1 || (g->precompute_intercepts && g->intercept_offset))
+    const int max_edges = ctx.cfg->one_launch_max_edges == 0 ? CLUSTER_MAX_EDGES : ctx.cfg->one_launch_max_edges;
+    if (E < 1 || E > max_edges || N < 1 || (g->precompute_intercepts && g->intercept_offset))
         return Status::Ok();
     const long long S = g->adj_offset[N];
     if (g->adj_offset[0] != 0 || S < 0) return Status::Ok();      // fit_graph reports it

@@ -233,7 +233,8 @@ def last_fit_stats():
     lib().dressx_last_fit_stats(ctypes.byref(st))
     return dict(common_terms=st.common_terms, sweeps=st.sweeps, setup_ms=st.setup_ms, iterate_ms=st.iterate_ms,
                 vertex_bins=list(zip(st.vertex_bin_items, st.vertex_bin_terms)),
-                edge_bins=list(zip(st.edge_bin_items, st.edge_bin_terms)))
+                edge_bins=list(zip(st.edge_bin_items, st.edge_bin_terms)),
+                phases_ms=dict(zip(("upload", "validate", "pairs_and_bins", "renumber", "download"), st.phase_ms)))
 
 
 def dress_cuda(N, E, U, V, W=None, NW=None, variant=UNDIRECTED, precompute_intercepts=0,
@@ -345,16 +346,20 @@ def nabla_fit_many(graphs, k=1, **kw):
     return [r[0] for r in hist_requests(graphs, NABLA, k, **kw)]
 
 
-def configure(device=-1, memory_budget_bytes=0, fit_chunk=0, group_threads=0, exact_sums=0):
+def configure(device=-1, memory_budget_bytes=0, fit_chunk=0, group_threads=0, exact_sums=0,
+              one_launch_max_edges=0):
     """Replace the engine configuration (``dressx_configure``).  exact_sums=1
     sends every sum through the sorted path that backs the certified sums
-    (same bits, slower); tests use it to exercise that path."""
+    (same bits, slower); tests use it to exercise that path.
+    one_launch_max_edges: graphs up to this many edges are fitted in one
+    launch (0 = the built-in limit, -1 = never)."""
     cfg = _abi.Config()
     cfg.device = int(device)
     cfg.memory_budget_bytes = int(memory_budget_bytes)
     cfg.fit_chunk = int(fit_chunk)
     cfg.group_threads = int(group_threads)
     cfg.exact_sums = int(exact_sums)
+    cfg.one_launch_max_edges = int(one_launch_max_edges)
     _check(lib().dressx_configure(ctypes.byref(cfg)))
 
 

@@ -53,7 +53,7 @@ class Config(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int), ("memory_budget_bytes", ctypes.c_size_t),
         ("fit_chunk", ctypes.c_int), ("group_threads", ctypes.c_int),
-        ("exact_sums", ctypes.c_int), ("reserved", ctypes.c_int * 7),
+        ("exact_sums", ctypes.c_int), ("one_launch_max_edges", ctypes.c_int), ("reserved", ctypes.c_int * 6),
     ]
 
 
@@ -61,7 +61,8 @@ class FitStats(ctypes.Structure):
     _fields_ = [("common_terms", ctypes.c_int64), ("sweeps", ctypes.c_int),
                 ("setup_ms", ctypes.c_double), ("iterate_ms", ctypes.c_double),
                 ("vertex_bin_items", ctypes.c_int64 * 8), ("vertex_bin_terms", ctypes.c_int64 * 8),
-                ("edge_bin_items", ctypes.c_int64 * 8), ("edge_bin_terms", ctypes.c_int64 * 8)]
+                ("edge_bin_items", ctypes.c_int64 * 8), ("edge_bin_terms", ctypes.c_int64 * 8),
+                ("phase_ms", ctypes.c_double * 5)]
 
 
 class ServerConfig(ctypes.Structure):

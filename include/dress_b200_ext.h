@@ -41,7 +41,10 @@ typedef struct dressx_config_t {
     int     exact_sums;           /* 1 = every sum takes the sorted path (the
                                      fallback of the certified sums; slower,
                                      same bits); for testing that path        */
-    int     reserved[7];
+    int     one_launch_max_edges; /* graphs up to this many edges are fitted
+                                     in one launch; 0 = built-in limit,
+                                     -1 = never                               */
+    int     reserved[6];
 } dressx_config_t;
 
 /* Replace the engine configuration; call before the first fit. */
@@ -64,6 +67,9 @@ typedef struct dressx_fit_stats_t {
      * <=4096, more terms), vertices (row slots) and edges (common pairs) */
     int64_t vertex_bin_items[8], vertex_bin_terms[8];
     int64_t edge_bin_items[8], edge_bin_terms[8];
+    /* host time of the phases: upload, validation, common-neighbour tables
+     * and bins, renumbering and sweep set-up, download of the results */
+    double  phase_ms[5];
 } dressx_fit_stats_t;
 int dressx_last_fit_stats(dressx_fit_stats_t *out);
 
