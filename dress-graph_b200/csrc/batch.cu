@@ -19,6 +19,10 @@
 //     request's value segment (the histogram is built afterwards, hist.cu).
 #include <cooperative_groups.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "batch.h"
 #include "common.cuh"
 
@@ -234,7 +238,8 @@ __device__ __forceinline__ int group_sum(const ClusterGroup &g, int v, double *,
 // of its endpoints' lookup against the deleted vertices.
 template <class Arr>
 struct RowTerms {
-    View G;
+    const int *row_eid, *U, *V;
+    const double *w;
     Mask mk;
     Arr d0;
     const unsigned *eb;
@@ -242,9 +247,9 @@ struct RowTerms {
     bool delta;
     __device__ __forceinline__ bool operator()(int j, double &t) const
     {
-        const int e = G.row_eid[rb + j];
-        if (delta && !(eb ? ((eb[e >> 5] >> (e & 31)) & 1u) != 0 : mk.alive(G.U[e] + G.V[e] - u))) return false;
-        t = dmul(G.w[e], d0[e]);
+        const int e = row_eid[rb + j];
+        if (delta && !(eb ? ((eb[e >> 5] >> (e & 31)) & 1u) != 0 : mk.alive(U[e] + V[e] - u))) return false;
+        t = dmul(w[e], d0[e]);
         return true;
     }
 };
@@ -253,7 +258,9 @@ struct RowTerms {
 // pair whose (u, x) edge is live (dress.c:485-490)
 template <class Arr>
 struct PairTerms {
-    View G;
+    const int2 *pairs;
+    const int *U, *V;
+    const double *w;
     Mask mk;
     Arr d0;
     const unsigned *eb;
@@ -261,10 +268,10 @@ struct PairTerms {
     bool delta;
     __device__ __forceinline__ bool operator()(int j, double &t) const
     {
-        const int2 pr = G.pairs[pb + j];
-        if (delta && !(eb ? ((eb[pr.x >> 5] >> (pr.x & 31)) & 1u) != 0 : mk.alive(G.U[pr.x] + G.V[pr.x] - u)))
+        const int2 pr = pairs[pb + j];
+        if (delta && !(eb ? ((eb[pr.x >> 5] >> (pr.x & 31)) & 1u) != 0 : mk.alive(U[pr.x] + V[pr.x] - u)))
             return false;
-        t = dadd(dmul(G.w[pr.x], d0[pr.x]), dmul(G.w[pr.y], d0[pr.y]));
+        t = dadd(dmul(w[pr.x], d0[pr.x]), dmul(w[pr.y], d0[pr.y]));
         return true;
     }
 };
@@ -334,7 +341,7 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
         for (int u = g.t; u < N; u += g.size) {
             if (!mk.alive(u)) continue;
             const int rb = G.row_off[u], deg = G.row_off[u + 1] - rb;
-            const RowTerms<Arr> rt{G, mk, d0, bits ? eb : nullptr, rb, u, P.kind == ITEM_DELTA};
+            const RowTerms<Arr> rt{G.row_eid, G.U, G.V, G.w, mk, d0, bits ? eb : nullptr, rb, u, P.kind == ITEM_DELTA};
             vd[u] = dsqrt(item_sum(dmul(4.0, mk.weight(u, G.nw)), deg, rt, P.force_exact != 0));
         }
         g.sync();
@@ -347,7 +354,7 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
             const double a4u = dmul(4.0, mk.weight(u, G.nw));
             const double self = P.fwd ? dadd(a4u, own) : dadd(dadd(a4u, dmul(4.0, mk.weight(v, G.nw))), dmul(2.0, own));
             const int pb = G.ioff[e], np = G.ioff[e + 1] - pb;
-            const PairTerms<Arr> pt{G, mk, d0, bits ? eb : nullptr, pb, u, P.kind == ITEM_DELTA};
+            const PairTerms<Arr> pt{G.pairs, G.U, G.V, G.w, mk, d0, bits ? eb : nullptr, pb, u, P.kind == ITEM_DELTA};
             const double num = item_sum(self, np, pt, P.force_exact != 0);
             const double den = dmul(vd[u], vd[v]);
             const double r = den > 0.0 ? ddiv(num, den) : 0.0;
@@ -562,8 +569,30 @@ Status launch_cluster_m(const ParentDesc *d_parent, int E, int N, int lnc, int s
     const int per_e = ((E + span - 1) / span) * CL_THREADS, per_n = ((N + span - 1) / span) * CL_THREADS;
     const size_t smem = (size_t)(2 * per_e + per_n + 2 * (CL_THREADS / 32) + 2) * sizeof(double) +
                         4 * CL_MAX_CTAS * sizeof(double *);
-    DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (nc > 8) DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    // attributes and the placement check are set up once per device and
+    // cluster shape: the queries cost more than a small fit's whole launch
+    int dev = 0;
+    DRESS_CUDA_TRY(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, size_t>, int> placeable;      // (device, CTAs, smem) -> clusters
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = placeable.find(std::make_tuple(dev, nc, smem));
+        if (it != placeable.end()) {
+            if (it->second < 1) return Status::Err(DRESSX_EUNSUPPORTED, "cluster fit does not fit the device");
+        }
+    }
+    static std::mutex amu;
+    static std::map<int, size_t> attr_smem;                             // device -> dynamic smem set
+    {
+        std::lock_guard<std::mutex> lk(amu);
+        size_t &have = attr_smem[dev];
+        if (have < smem) {
+            DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            DRESS_CUDA_TRY(cudaFuncSetAttribute(k_fit_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            have = smem;
+        }
+    }
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3((unsigned)nc);
     cfg.blockDim = dim3(CL_THREADS);
@@ -576,11 +605,21 @@ Status launch_cluster_m(const ParentDesc *d_parent, int E, int N, int lnc, int s
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    int clusters = 0;
-    if (cudaOccupancyMaxActiveClusters(&clusters, k_fit_cluster, &cfg) != cudaSuccess || clusters < 1) {
-        cudaGetLastError();
-        return Status::Err(DRESSX_EUNSUPPORTED, "cluster fit does not fit the device");
+    int clusters = -1;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = placeable.find(std::make_tuple(dev, nc, smem));
+        if (it != placeable.end()) clusters = it->second;
     }
+    if (clusters < 0) {
+        if (cudaOccupancyMaxActiveClusters(&clusters, k_fit_cluster, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            clusters = 0;
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        placeable[std::make_tuple(dev, nc, smem)] = clusters;
+    }
+    if (clusters < 1) return Status::Err(DRESSX_EUNSUPPORTED, "cluster fit does not fit the device");
     count_launch();
     DRESS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_fit_cluster, d_parent, per_e, per_n, lnc));
     (void)sms;

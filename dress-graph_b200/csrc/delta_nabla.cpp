@@ -63,6 +63,48 @@ void merge_walk_pairs(p_dress_graph_t g, std::vector<int> &ioff, std::vector<int
     }
     ioff.assign((size_t)E + 1, 0);
     pairs.clear();
+    if (!dup) {
+        // Rows without repeated neighbours: the intersection of rows U[e]
+        // and V[e] is found by marking U[e]'s row and scanning V[e]'s in
+        // order -- the merge walk's pairs, in its order (ascending common
+        // neighbour), without its branches.  Edges are taken grouped by
+        // U[e], so a row is marked once.
+        std::vector<int> first((size_t)N + 1, 0), byu((size_t)E), slot_of((size_t)N), stamp((size_t)N, -1);
+        for (int e = 0; e < E; ++e) ++first[(size_t)g->U[e] + 1];
+        for (int u = 0; u < N; ++u) first[(size_t)u + 1] += first[(size_t)u];
+        {
+            std::vector<int> cur(first.begin(), first.end() - 1);
+            for (int e = 0; e < E; ++e) byu[(size_t)cur[(size_t)g->U[e]]++] = e;
+        }
+        std::vector<int> cnt((size_t)E, 0);
+        std::vector<std::pair<int, int>> tmp;
+        std::vector<long long> at((size_t)E, -1);
+        for (int u = 0; u < N; ++u) {
+            if (first[(size_t)u] == first[(size_t)u + 1]) continue;
+            for (int s = off[u]; s < off[u + 1]; ++s) {
+                stamp[(size_t)tg[s]] = u;
+                slot_of[(size_t)tg[s]] = s;
+            }
+            for (int q = first[(size_t)u]; q < first[(size_t)u + 1]; ++q) {
+                const int e = byu[(size_t)q], v = g->V[e];
+                at[(size_t)e] = (long long)tmp.size();
+                for (int s = off[v]; s < off[v + 1]; ++s) {
+                    const int x = tg[s];
+                    if (stamp[(size_t)x] == u) tmp.emplace_back(ei[slot_of[(size_t)x]], ei[s]);
+                }
+                cnt[(size_t)e] = (int)((long long)tmp.size() - at[(size_t)e]);
+            }
+        }
+        for (int e = 0; e < E; ++e) ioff[(size_t)e + 1] = ioff[(size_t)e] + cnt[(size_t)e];
+        pairs.resize(2 * tmp.size());
+        for (int e = 0; e < E; ++e)
+            for (int k = 0; k < cnt[(size_t)e]; ++k) {
+                const auto &pr = tmp[(size_t)(at[(size_t)e] + k)];
+                pairs[2 * ((size_t)ioff[(size_t)e] + k)] = pr.first;
+                pairs[2 * ((size_t)ioff[(size_t)e] + k) + 1] = pr.second;
+            }
+        return;
+    }
     for (int e = 0; e < E; ++e) {
         int iu = off[g->U[e]], iu_end = off[g->U[e] + 1];
         int iv = off[g->V[e]], iv_end = off[g->V[e] + 1];

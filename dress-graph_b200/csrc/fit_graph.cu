@@ -572,6 +572,15 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     }
     vb.start[NB] = N;
     eb.start[NB] = E;
+    // the warp bin, longest first, split where items have at most 256 and 64 terms
+    for (int side = 0; side < 2; ++side) {
+        Bins &bb = side ? eb : vb;
+        const int base = side ? NF : 0;
+        bb.med[0] = bb.start[BMED];
+        bb.med[1] = cur[base + fine_of(256)];
+        bb.med[2] = cur[base + fine_of(64)];
+        bb.med[3] = bb.start[BMED + 1];
+    }
     DRESS_CUDA_TRY(counted_memcpy(d_bc.get() + 2 * NF, cur.data(), 2 * NF * sizeof(int), cudaMemcpyHostToDevice, st));
     count_launch(), k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), d_bc.get() + 2 * NF, d_vperm.get(), d_vinv.get());
     // Edges of a large graph: one stable radix sort on (fine bin, owner,

@@ -14,6 +14,7 @@
 // k_fit_cluster).  Larger graphs, and graphs that carry their own intercept
 // tables, take the multi-kernel fit in fit_graph.cu.
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cstring>
 #include <vector>
@@ -61,6 +62,83 @@ bool small_graph_ok(p_dress_graph_t g, int &maxdeg)
         if (g->U[e] < 0 || g->U[e] >= N || g->V[e] < 0 || g->V[e] >= N) return false;
     return true;
 }
+
+// Common-neighbour pairs of a graph for the cluster fit, on the device: one
+// block.  Each thread runs the reference's merge walk (dress.c:500-529) over
+// the rows of its edges -- counts first, then a block scan of the counts
+// into the offsets, then the same walk writes the pairs, in the walk's
+// order.  Rows and offsets are staged in shared memory when they fit.
+constexpr int PAIR_THR = 1024;
+
+__global__ void __launch_bounds__(PAIR_THR) k_small_pairs(int N, int E, const int *off_g, const int *tgt_g,
+                                                          const int *eidx, const int *U, const int *V, int *ioff,
+                                                          int2 *pairs, int staged)
+{
+    extern __shared__ __align__(16) int sm[];
+    __shared__ int part[PAIR_THR / 32];
+    const int *off = off_g, *tgt = tgt_g;
+    const long long S = off_g[N];
+    if (staged) {
+        int *so = sm, *st = sm + N + 1;
+        for (int i = threadIdx.x; i <= N; i += blockDim.x) so[i] = off_g[i];
+        for (long long i = threadIdx.x; i < S; i += blockDim.x) st[i] = tgt_g[i];
+        __syncthreads();
+        off = so;
+        tgt = st;
+    }
+    // this thread's edges: a contiguous chunk, so the scan is a chunk sum
+    const int per = (E + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int e0 = min(E, (int)threadIdx.x * per), e1 = min(E, e0 + per);
+    int mine = 0;
+    for (int e = e0; e < e1; ++e) {
+        int iu = off[U[e]], iu_end = off[U[e] + 1];
+        int iv = off[V[e]], iv_end = off[V[e] + 1];
+        int c = 0;
+        while (iu < iu_end && iv < iv_end) {
+            const int x = tgt[iu], y = tgt[iv];
+            c += x == y;
+            iu += (x <= y);
+            iv += (x >= y);
+        }
+        ioff[e + 1] = c;          // counts for now
+        mine += c;
+    }
+    // exclusive block scan of the chunk sums
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) part[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int v = lane < (int)(blockDim.x >> 5) ? part[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        if (lane < (int)(blockDim.x >> 5)) part[lane] = v;
+    }
+    __syncthreads();
+    int base = incl - mine + (wid > 0 ? part[wid - 1] : 0);
+    if (threadIdx.x == 0) ioff[0] = 0;
+    for (int e = e0; e < e1; ++e) {
+        const int c = ioff[e + 1];
+        int iu = off[U[e]], iu_end = off[U[e] + 1];
+        int iv = off[V[e]], iv_end = off[V[e] + 1];
+        int q = base;
+        while (iu < iu_end && iv < iv_end) {
+            const int x = tgt[iu], y = tgt[iv];
+            if (x == y) pairs[q++] = make_int2(eidx[iu], eidx[iv]);
+            iu += (x <= y);
+            iv += (x >= y);
+        }
+        base += c;
+        ioff[e + 1] = base;
+    }
+}
+
 }  // namespace
 
 Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *iterations, double *delta,
@@ -94,12 +172,25 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     if (!small_graph_ok(g, maxdeg)) return Status::Ok();       // fit_graph reports it
     if (maxdeg > SMALL_MAX_DEG) return Status::Ok();
 
+    // the common-neighbour pairs: on the host for one CTA (whose staged
+    // image must be exact), on the device for a cluster, in an image sized
+    // for the bound T <= sum_e min(deg u, deg v)
     std::vector<int> ioff, pairs;
-    bool dup = false;                        // repeated neighbours: the merge walk pairs them as the reference does
-    merge_walk_pairs(g, ioff, pairs, maxdeg, dup);
-    const int T = (int)(pairs.size() / 2);
+    long long T = 0;
+    if (one_cta) {
+        bool dup = false;                    // repeated neighbours: the merge walk pairs them as the reference does
+        merge_walk_pairs(g, ioff, pairs, maxdeg, dup);
+        T = (long long)(pairs.size() / 2);
+    } else {
+        for (int e = 0; e < E; ++e) {
+            const int du = g->adj_offset[g->U[e] + 1] - g->adj_offset[g->U[e]];
+            const int dv = g->adj_offset[g->V[e] + 1] - g->adj_offset[g->V[e]];
+            T += du < dv ? du : dv;
+        }
+        if (T > INT_MAX / 2) return Status::Ok();
+    }
     const int has_nw = g->NW != nullptr;
-    const ParentLayout PL = parent_layout(N, E, (int)S, T, has_nw, 1);
+    const ParentLayout PL = parent_layout(N, E, (int)S, (int)T, has_nw, 1);
 
     BatchLaunch L{};
     L.gsize = SMALL_GSIZE;
@@ -131,8 +222,10 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     std::memcpy(b + PL.w, g->edge_weight, (size_t)E * 8);
     std::memcpy(b + PL.row_off, g->adj_offset, (size_t)(N + 1) * 4);
     if (S) std::memcpy(b + PL.row_eid, g->adj_edge_idx, (size_t)S * 4);
-    std::memcpy(b + PL.ioff, ioff.data(), (size_t)(E + 1) * 4);
-    if (T) std::memcpy(b + PL.pairs, pairs.data(), (size_t)T * 8);
+    if (one_cta) {
+        std::memcpy(b + PL.ioff, ioff.data(), (size_t)(E + 1) * 4);
+        if (T) std::memcpy(b + PL.pairs, pairs.data(), (size_t)T * 8);
+    }
     if (has_nw) std::memcpy(b + PL.nw, g->NW, (size_t)N * 8);
     std::memcpy(b + PL.dinit, g->edge_dress, (size_t)E * 8);
 
@@ -153,7 +246,7 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     P.N = N;
     P.E = E;
     P.S = (int)S;
-    P.T = T;
+    P.T = (int)T;
     P.kind = ITEM_PLAIN;
     P.k = 0;
     P.fwd = g->variant == DRESS_VARIANT_FORWARD || g->variant == DRESS_VARIANT_BACKWARD;
@@ -169,6 +262,23 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     P.stride = 1;
     const Chunk ch{0, 1, 0};
     DRESS_CUDA_TRY(counted_memcpy(d_data.get(), packed.data(), packed.size(), cudaMemcpyHostToDevice, st));
+    DevBuf<int> d_tgt;
+    if (!one_cta) {
+        DRESS_TRY(d_tgt.alloc((size_t)S, st));
+        DRESS_CUDA_TRY(counted_memcpy(d_tgt.get(), g->adj_target, (size_t)S * sizeof(int), cudaMemcpyHostToDevice, st));
+        unsigned char *dd = d_data.get();
+        const size_t pair_smem = (size_t)(N + 1 + S) * sizeof(int);
+        const int staged = pair_smem <= (size_t)smem_cap ? 1 : 0;
+        static bool attr_set[64] = {};
+        if (staged && ctx.device >= 0 && ctx.device < 64 && !attr_set[ctx.device]) {
+            DRESS_CUDA_TRY(cudaFuncSetAttribute(k_small_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap));
+            attr_set[ctx.device] = true;
+        }
+        count_launch(), k_small_pairs<<<1, PAIR_THR, staged ? pair_smem : 0, st>>>(
+            N, E, (const int *)(dd + PL.row_off), d_tgt.get(), (const int *)(dd + PL.row_eid),
+            (const int *)(dd + PL.U), (const int *)(dd + PL.V), (int *)(dd + PL.ioff), (int2 *)(dd + PL.pairs), staged);
+        DRESS_CUDA_TRY(cudaGetLastError());
+    }
     DRESS_CUDA_TRY(counted_memcpy(d_desc.get(), &P, sizeof P, cudaMemcpyHostToDevice, st));
     DRESS_CUDA_TRY(counted_memcpy(d_chunk.get(), &ch, sizeof ch, cudaMemcpyHostToDevice, st));
     DRESS_CUDA_TRY(cudaMemsetAsync(d_stats.get(), 0, ST_WORDS * sizeof(unsigned long long), st));

@@ -107,6 +107,65 @@ __global__ void __launch_bounds__(RADIX) k_seg_offsets(const long long *seg_begi
     }
 }
 
+// The same offsets for one long segment, in parallel: per chunk of
+// OFF_CHUNK tiles the digit sums (k_chunk_sums), then the digit bases and
+// every chunk's base per digit (k_chunk_bases, one block over the chunks),
+// then each chunk's tiles (k_chunk_fill).  k_seg_offsets walks every tile of
+// its segment with one block, which makes a segment of 10^8 keys (12K tiles)
+// cost milliseconds per pass.
+constexpr int OFF_CHUNK = 64;
+
+__global__ void __launch_bounds__(RADIX) k_chunk_sums(int nt, const int *counts, long long *csum)
+{
+    const int c = blockIdx.x, d = threadIdx.x;
+    const int t1 = min(nt, (c + 1) * OFF_CHUNK);
+    long long sum = 0;
+    for (int t = c * OFF_CHUNK; t < t1; ++t) sum += counts[(long long)t * RADIX + d];
+    csum[(long long)c * RADIX + d] = sum;
+}
+
+__global__ void __launch_bounds__(RADIX) k_chunk_bases(int nch, const long long *seg_begin, long long *csum,
+                                                       int *moves)
+{
+    __shared__ long long base[RADIX];
+    __shared__ int nonzero;
+    const int d = threadIdx.x;
+    long long tot = 0;
+    for (int c = 0; c < nch; ++c) tot += csum[(long long)c * RADIX + d];
+    if (d == 0) nonzero = 0;
+    base[d] = tot;
+    __syncthreads();
+    if (tot > 0) atomicAdd(&nonzero, 1);
+    if (d == 0) {
+        long long run = seg_begin[0];
+        for (int k = 0; k < RADIX; ++k) {
+            const long long c = base[k];
+            base[k] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (nonzero > 1 && d == 0) *moves = 1;
+    long long run = base[d];
+    for (int c = 0; c < nch; ++c) {
+        const long long v = csum[(long long)c * RADIX + d];
+        csum[(long long)c * RADIX + d] = run;
+        run += v;
+    }
+}
+
+__global__ void __launch_bounds__(RADIX) k_chunk_fill(int nt, const int *counts, const long long *cbase,
+                                                      long long *offs)
+{
+    const int c = blockIdx.x, d = threadIdx.x;
+    const int t1 = min(nt, (c + 1) * OFF_CHUNK);
+    long long run = cbase[(long long)c * RADIX + d];
+    for (int t = c * OFF_CHUNK; t < t1; ++t) {
+        offs[(long long)t * RADIX + d] = run;
+        run += counts[(long long)t * RADIX + d];
+    }
+}
+
 // stable scatter of one tile: rounds of HT consecutive keys, each key ranked
 // by (its rank among equal digits in its warp) + (same digit in earlier warps
 // of the round) + (same digit in earlier rounds of the tile)
@@ -290,12 +349,22 @@ Status sort_segments(unsigned long long *keys, unsigned long long *alt, const st
             hi - lo, keys + lo);
     unsigned long long *a = keys, *b = alt;
     unsigned *pa = vals, *pb = valt;
+    const bool chunked = nseg == 1 && nt >= 4 * OFF_CHUNK;
+    const int nch = (nt + OFF_CHUNK - 1) / OFF_CHUNK;
+    DevBuf<long long> d_csum;
+    if (chunked) DRESS_TRY(d_csum.alloc((size_t)nch * RADIX, st));
     for (int pass = 0; pass < 8; ++pass) {
         int shift = 8 * pass;
         count_launch(), k_tile_hist<<<nt, HT, 0, st>>>(sp.tiles.get(), a, shift, d_counts.get());
         DRESS_CUDA_TRY(cudaMemsetAsync(d_moves.get(), 0, sizeof(int), st));
-        count_launch(), k_seg_offsets<<<nseg, RADIX, 0, st>>>(sp.seg_begin.get(), d_seg_tile0.get(), d_counts.get(),
-                                                              d_offs.get(), d_moves.get());
+        if (chunked) {
+            count_launch(), k_chunk_sums<<<nch, RADIX, 0, st>>>(nt, d_counts.get(), d_csum.get());
+            count_launch(), k_chunk_bases<<<1, RADIX, 0, st>>>(nch, sp.seg_begin.get(), d_csum.get(), d_moves.get());
+            count_launch(), k_chunk_fill<<<nch, RADIX, 0, st>>>(nt, d_counts.get(), d_csum.get(), d_offs.get());
+        } else {
+            count_launch(), k_seg_offsets<<<nseg, RADIX, 0, st>>>(sp.seg_begin.get(), d_seg_tile0.get(),
+                                                                  d_counts.get(), d_offs.get(), d_moves.get());
+        }
         int moves = 0;
         DRESS_CUDA_TRY(counted_memcpy(&moves, d_moves.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));

@@ -18,7 +18,8 @@
 // order is kept between sweeps.
 //
 //   bins: 0 stored terms; <=2, <=4, <=8, <=16 (one thread per item);
-//   <=MED_CAP (one warp per item); more (one block per item, largest first).
+//   <=MED_CAP (a group of 8, 16 or 32 lanes per item); <=BIG_CAP (a warp per
+//   item); more (one block per item, largest first).
 #pragma once
 #include <algorithm>
 #include <climits>
@@ -232,26 +233,38 @@ __global__ void __launch_bounds__(THR) k_edge_thr(Sweep s, int begin, int end)
     block_max_to(max_slot(s), lmax);
 }
 
-// ---- one warp per item ----------------------------------------------------------------
+// ---- a group of GW lanes per item ------------------------------------------------------
+// The warp bin (17..MED_CAP terms) is split by term count into groups of 8,
+// 16 or 32 lanes per item (at most 8 or 16 terms a lane in the smaller
+// ones): fewer idle lanes and merge rounds for short items.  A warp takes
+// 32 / GW consecutive items per step, so the loop control and the lane
+// merge stay warp-uniform.
 
 constexpr int WARP_THR = 256;
 
-template <bool UNIF>
-__global__ void __launch_bounds__(WARP_THR) k_vertex_warp(Sweep s, int begin, int end)
+template <bool UNIF, int GW>
+__global__ void __launch_bounds__(WARP_THR) k_vertex_grp(Sweep s, int begin, int end)
 {
     if (skipped(s)) return;
-    const int lane = threadIdx.x & 31;
+    constexpr int IPW = 32 / GW;                  // items per warp step
+    const int lane = threadIdx.x & (GW - 1);
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < end; i += nwarps) {
-        const long long rb = s.row_off[i];
-        const int deg = (int)(s.row_off[i + 1] - rb);
+    for (int i0 = begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * IPW; i0 < end; i0 += nwarps * IPW) {
+        const int i = i0 + (int)((threadIdx.x & 31) / GW);
+        const bool valid = i < end;
+        long long rb = 0;
+        int deg = 0;
+        if (valid) {
+            rb = s.row_off[i];
+            deg = (int)(s.row_off[i + 1] - rb);
+        }
         const int *re = s.row_eid + rb;
         CSum q;
         q.init();
-        if (lane == 0) q.add(four_nw(s, i));
+        if (valid && lane == 0) q.add(four_nw(s, i));
         int k = lane;
-        for (; k + 96 < deg; k += 128) {
-            const int e0 = re[k], e1 = re[k + 32], e2 = re[k + 64], e3 = re[k + 96];
+        for (; k + 3 * GW < deg; k += 4 * GW) {
+            const int e0 = re[k], e1 = re[k + GW], e2 = re[k + 2 * GW], e3 = re[k + 3 * GW];
             const double t0 = prod<UNIF>(s, e0), t1 = prod<UNIF>(s, e1);
             const double t2 = prod<UNIF>(s, e2), t3 = prod<UNIF>(s, e3);
             q.add(t0);
@@ -259,9 +272,9 @@ __global__ void __launch_bounds__(WARP_THR) k_vertex_warp(Sweep s, int begin, in
             q.add(t2);
             q.add(t3);
         }
-        for (; k < deg; k += 32) q.add(prod<UNIF>(s, re[k]));
-        q.merge_lanes(32);
-        if (lane == 0) {
+        for (; k < deg; k += GW) q.add(prod<UNIF>(s, re[k]));
+        q.merge_lanes(GW);
+        if (valid && lane == 0) {
             double sum;
             if (!s.force_exact && q.result(sum)) s.vd[i] = dsqrt(sum);
             else queue_item(s.qv, &s.qcount[0], i);
@@ -269,30 +282,37 @@ __global__ void __launch_bounds__(WARP_THR) k_vertex_warp(Sweep s, int begin, in
     }
 }
 
-template <bool UNIF>
-__global__ void __launch_bounds__(WARP_THR) k_edge_warp(Sweep s, int begin, int end)
+template <bool UNIF, int GW>
+__global__ void __launch_bounds__(WARP_THR) k_edge_grp(Sweep s, int begin, int end)
 {
     if (skipped(s)) return;
-    const int lane = threadIdx.x & 31;
+    constexpr int IPW = 32 / GW;
+    const int lane = threadIdx.x & (GW - 1);
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     double lmax = 0.0;
-    for (int j = begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); j < end; j += nwarps) {
-        const long long pb = s.ioff[j];
-        const int n = (int)(s.ioff[j + 1] - pb);
+    for (int j0 = begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * IPW; j0 < end; j0 += nwarps * IPW) {
+        const int j = j0 + (int)((threadIdx.x & 31) / GW);
+        const bool valid = j < end;
+        long long pb = 0;
+        int n = 0;
+        if (valid) {
+            pb = s.ioff[j];
+            n = (int)(s.ioff[j + 1] - pb);
+        }
         const int2 *pp = s.pairs + pb;
         int u = 0, v = 0;
         double dj = 0.0;
         CSum q;
         q.init();
-        if (lane == 0) {
+        if (valid && lane == 0) {
             u = s.eu[j];
             v = s.ev[j];
             dj = s.d[j];
             q.add(self_term(s, u, v, own_prod<UNIF>(s, j, dj)));
         }
         int k = lane;
-        for (; k + 96 < n; k += 128) {
-            const int2 p0 = pp[k], p1 = pp[k + 32], p2 = pp[k + 64], p3 = pp[k + 96];
+        for (; k + 3 * GW < n; k += 4 * GW) {
+            const int2 p0 = pp[k], p1 = pp[k + GW], p2 = pp[k + 2 * GW], p3 = pp[k + 3 * GW];
             const double t0 = pair_term<UNIF>(s, p0), t1 = pair_term<UNIF>(s, p1);
             const double t2 = pair_term<UNIF>(s, p2), t3 = pair_term<UNIF>(s, p3);
             q.add(t0);
@@ -300,9 +320,9 @@ __global__ void __launch_bounds__(WARP_THR) k_edge_warp(Sweep s, int begin, int 
             q.add(t2);
             q.add(t3);
         }
-        for (; k < n; k += 32) q.add(pair_term<UNIF>(s, pp[k]));
-        q.merge_lanes(32);
-        if (lane == 0) {
+        for (; k < n; k += GW) q.add(pair_term<UNIF>(s, pp[k]));
+        q.merge_lanes(GW);
+        if (valid && lane == 0) {
             double num;
             if (!s.force_exact && q.result(num)) lmax = fmax(lmax, finish_edge<UNIF>(s, j, u, v, dj, num));
             else queue_item(s.qe, &s.qcount[1], j);
@@ -475,6 +495,7 @@ __global__ void k_clear_queues(unsigned *qcount)
 
 struct Bins {
     int start[NB + 1];
+    int med[4];                    // the warp bin split by term count (see launch_phase)
     bool has(int b) const { return start[b + 1] > start[b]; }
     int count(int b) const { return start[b + 1] - start[b]; }
 };
@@ -510,22 +531,47 @@ Status set_sweep_attributes(size_t exact_smem)
 template <bool UNIF, bool EDGE>
 Status launch_phase(const Sweep &s, const Bins &b, const LaunchCfg &c)
 {
-    const bool blocks = b.has(BBLOCK) || b.has(BBIG);
+    // items beyond BIG_CAP terms: a block each, on the side stream
+    const bool blocks = b.has(BBIG);
     if (blocks) {
         DRESS_CUDA_TRY(cudaEventRecord(c.fork, c.st));
         DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
-        const int lo = b.start[BBLOCK], hi = b.start[BBIG + 1];
+        const int lo = b.start[BBIG], hi = b.start[BBIG + 1];
         const unsigned g = grid_for(hi - lo, 1, 8LL * c.sms);
         count_launch();
         if (EDGE) k_edge_blk<UNIF><<<g, BLK_THR, 0, c.side>>>(s, lo, hi);
         else k_vertex_blk<UNIF><<<g, BLK_THR, 0, c.side>>>(s, lo, hi);
     }
-    if (b.has(BMED)) {
-        const int lo = b.start[BMED], hi = b.start[BMED + 1];
+    // MED_CAP..BIG_CAP terms: a warp each (16 to 128 terms a lane)
+    if (b.has(BBLOCK)) {
+        const int lo = b.start[BBLOCK], hi = b.start[BBLOCK + 1];
         const unsigned g = grid_for((long long)(hi - lo) * 32, WARP_THR, 16LL * c.sms);
         count_launch();
-        if (EDGE) k_edge_warp<UNIF><<<g, WARP_THR, 0, c.st>>>(s, lo, hi);
-        else k_vertex_warp<UNIF><<<g, WARP_THR, 0, c.st>>>(s, lo, hi);
+        if (EDGE) k_edge_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, lo, hi);
+        else k_vertex_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, lo, hi);
+    }
+    if (b.has(BMED)) {
+        // [med[0], med[1]): more than 256 terms, [med[1], med[2]): 65..256,
+        // [med[2], med[3]): 17..64 (the bin is ordered longest first)
+        const int *m = b.med;
+        if (m[1] > m[0]) {
+            const unsigned g = grid_for((long long)(m[1] - m[0]) * 32, WARP_THR, 16LL * c.sms);
+            count_launch();
+            if (EDGE) k_edge_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, m[0], m[1]);
+            else k_vertex_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, m[0], m[1]);
+        }
+        if (m[2] > m[1]) {
+            const unsigned g = grid_for((long long)(m[2] - m[1]) * 16, WARP_THR, 16LL * c.sms);
+            count_launch();
+            if (EDGE) k_edge_grp<UNIF, 16><<<g, WARP_THR, 0, c.st>>>(s, m[1], m[2]);
+            else k_vertex_grp<UNIF, 16><<<g, WARP_THR, 0, c.st>>>(s, m[1], m[2]);
+        }
+        if (m[3] > m[2]) {
+            const unsigned g = grid_for((long long)(m[3] - m[2]) * 8, WARP_THR, 16LL * c.sms);
+            count_launch();
+            if (EDGE) k_edge_grp<UNIF, 8><<<g, WARP_THR, 0, c.st>>>(s, m[2], m[3]);
+            else k_vertex_grp<UNIF, 8><<<g, WARP_THR, 0, c.st>>>(s, m[2], m[3]);
+        }
     }
     if (EDGE) {
         // edges without common neighbours, then the thread bins with pairs
