@@ -254,33 +254,58 @@ __global__ void k_bin_scatter(int n, const int *len, int *cursor, int *perm, int
     }
 }
 
-// Sort keys of the edge renumbering.  Fine bin first (so every bin is one
-// contiguous range); block bins then largest first (the longest sums start
-// first); thread and warp bins by owner -- the endpoint of lower (degree, id)
-// rank, the triangle listing's orientation -- in the new vertex numbering,
-// then by the other endpoint.  A vertex owns most edges of its row unless it
-// is a hub, so its row's edges, and the (u, x) edges of the common-neighbour
-// pairs of its edges, sit next to each other: neighbouring lanes gather
-// neighbouring products.
-__global__ void k_edge_keys(int E, int N, const int *U, const int *V, const int *deg, const int *vinv,
-                            const int *cnt, unsigned long long *keys, unsigned *vals)
+// Sort keys of the edge renumbering of a large graph: the edges without
+// common neighbours first, then the others; within each part by owner -- the
+// endpoint of lower (degree, id) rank, the triangle listing's orientation --
+// in the new vertex numbering, then by the other endpoint.  A vertex owns
+// most edges of its row unless it is a hub, so a row's edges sit in two runs
+// and the (u, x) edges of an edge's common-neighbour pairs next to each
+// other: neighbouring lanes gather neighbouring products.
+__global__ void k_edge_keys(int E, const int *U, const int *V, const int *deg, const int *vinv, const int *cnt,
+                            unsigned long long *keys, unsigned *vals)
 {
-    const bool wide = N > (1 << 27);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        const int c = cnt[e];
-        const unsigned long long f = (unsigned long long)fine_of((long long)c);
-        unsigned long long low;
-        if (bin_of((long long)c) >= BBLOCK) {
-            low = (1ULL << 54) - 1 - (unsigned long long)c;
-        } else {
-            const int u = U[e], v = V[e];
-            const bool uo = rank_key(deg, u) <= rank_key(deg, v);
-            const unsigned long long o = (unsigned)vinv[uo ? u : v], x = (unsigned)vinv[uo ? v : u];
-            low = wide ? o : (o << 27) | x;
-        }
-        keys[e] = (f << 54) | low;
+        const int u = U[e], v = V[e];
+        const bool uo = rank_key(deg, u) <= rank_key(deg, v);
+        const unsigned long long o = (unsigned)vinv[uo ? u : v], x = (unsigned)vinv[uo ? v : u];
+        keys[e] = ((unsigned long long)(cnt[e] > 0) << 62) | (o << 31) | x;
         vals[e] = (unsigned)e;
     }
+}
+
+// size class of an edge with n > 0 common-neighbour pairs (the order of the
+// edge lists, see sweep::EdgeClasses)
+__device__ __forceinline__ unsigned pair_class(int n)
+{
+    return n <= 16 ? 0u : n <= 64 ? 3u : n <= 256 ? 2u : n <= MED_CAP ? 1u : n <= BIG_CAP ? 4u : 5u;
+}
+
+__global__ void k_class_keys(int e0, int E, const int *ncnt, unsigned long long *keys, unsigned *vals)
+{
+    for (int j = e0 + blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
+        keys[j - e0] = ((unsigned long long)pair_class(ncnt[j]) << 32) | (unsigned)j;
+        vals[j - e0] = (unsigned)j;
+    }
+}
+
+// bounds[c] = first position of class c in the sorted keys (c = 0..6)
+__global__ void k_class_bounds(int n, const unsigned long long *keys, int *bounds)
+{
+    const int c = threadIdx.x;
+    if (c > 6) return;
+    const unsigned long long want = (unsigned long long)c << 32;
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < want) lo = mid + 1;
+        else hi = mid;
+    }
+    bounds[c] = lo;
+}
+
+__global__ void k_iota(int n, int base, int *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = base + i;
 }
 
 __global__ void k_inverse(int n, const unsigned *perm, int *pinv, int *inv)
@@ -583,7 +608,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     }
     DRESS_CUDA_TRY(counted_memcpy(d_bc.get() + 2 * NF, cur.data(), 2 * NF * sizeof(int), cudaMemcpyHostToDevice, st));
     count_launch(), k_bin_scatter<<<vg, 256, 0, st>>>(N, d_deg.get(), d_bc.get() + 2 * NF, d_vperm.get(), d_vinv.get());
-    // Edges of a large graph: one stable radix sort on (fine bin, owner,
+    // Edges of a large graph: one stable radix sort on (any pairs, owner,
     // other endpoint), for the locality of the sweeps' gathers.  A small
     // graph's sweeps are bound by launch latency and its arrays sit in L2, so
     // it keeps the one-pass scatter (the sort's passes cost more than they save).
@@ -597,7 +622,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         DRESS_TRY(k1.alloc((size_t)E, st));
         DRESS_TRY(v0.alloc((size_t)E, st));
         DRESS_TRY(v1.alloc((size_t)E, st));
-        count_launch(), k_edge_keys<<<eg, 256, 0, st>>>(E, N, d_U.get(), d_V.get(), d_deg.get(), d_vinv.get(),
+        count_launch(), k_edge_keys<<<eg, 256, 0, st>>>(E, d_U.get(), d_V.get(), d_deg.get(), d_vinv.get(),
                                                         d_cnt.get(), k0.get(), v0.get());
         unsigned long long *sk = nullptr;
         unsigned *sv = nullptr;
@@ -662,6 +687,48 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
                                     uniform ? nullptr : d_pbuf.get(), d_ncnt.get());
     DRESS_TRY(d_ioff.alloc((size_t)E + 1, st));
     DRESS_TRY(exclusive_scan_i32(d_ncnt.get(), d_ioff.get(), E, d_scan_tmp.get(), st));
+    // The edges with common neighbours listed by size class (EdgeClasses):
+    // a large graph sorts their ids by class; a small one's bins are already
+    // in class order, so its list is their ids in order.
+    EdgeClasses ec{};
+    DevBuf<int> d_elist;
+    const int e0 = eb.count(B0);
+    ec.e0 = e0;
+    DRESS_TRY(d_elist.alloc((size_t)std::max(1, E - e0), st));
+    if (E - e0 > 0) {
+        if (locality) {
+            const int m = E - e0;
+            DevBuf<unsigned long long> k0, k1;
+            DevBuf<unsigned> v0, v1;
+            DevBuf<int> d_bounds;
+            DRESS_TRY(k0.alloc((size_t)m, st));
+            DRESS_TRY(k1.alloc((size_t)m, st));
+            DRESS_TRY(v0.alloc((size_t)m, st));
+            DRESS_TRY(v1.alloc((size_t)m, st));
+            DRESS_TRY(d_bounds.alloc(7, st));
+            count_launch(), k_class_keys<<<grid_for(m, 256, 32 * sms), 256, 0, st>>>(e0, E, d_ncnt.get(), k0.get(),
+                                                                                    v0.get());
+            unsigned long long *sk = nullptr;
+            unsigned *sv = nullptr;
+            DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), m, &sk, &sv, st, sms));
+            count_launch(), k_class_bounds<<<1, 32, 0, st>>>(m, sk, d_bounds.get());
+            DRESS_CUDA_TRY(cudaMemcpyAsync(d_elist.get(), sv, (size_t)m * sizeof(int), cudaMemcpyDeviceToDevice, st));
+            DRESS_CUDA_TRY(counted_memcpy(ec.cls, d_bounds.get(), 7 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+            ec.cls[6] = m;
+        } else {
+            count_launch(), k_iota<<<grid_for(E - e0, 256, 32 * sms), 256, 0, st>>>(E - e0, e0, d_elist.get());
+            const int b0 = e0;
+            ec.cls[0] = eb.start[B2] - b0;
+            ec.cls[1] = eb.start[BMED] - b0;
+            ec.cls[2] = eb.med[1] - b0;
+            ec.cls[3] = eb.med[2] - b0;
+            ec.cls[4] = eb.med[3] - b0;
+            ec.cls[5] = eb.start[BBIG] - b0;
+            ec.cls[6] = E - b0;
+        }
+    }
+    ec.list = d_elist.get();
     DRESS_TRY(d_pairs.alloc((size_t)(T > 0 ? T : 1), st));
     count_launch(), k_new_pairs<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_ioff_old.get(), d_pairs_old.get(), d_einv.get(),
                                     d_ioff.get(), d_pairs.get());
@@ -756,8 +823,8 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     }
     auto enqueue_pair = [&]() -> Status {
         for (int par = 0; par < 2; ++par) {
-            if (uniform) DRESS_TRY(launch_sweep<true>(sw2[par], vb, eb, lc));
-            else         DRESS_TRY(launch_sweep<false>(sw2[par], vb, eb, lc));
+            if (uniform) DRESS_TRY(launch_sweep<true>(sw2[par], vb, ec, lc));
+            else         DRESS_TRY(launch_sweep<false>(sw2[par], vb, ec, lc));
             count_launch(), k_next_sweep<<<1, 1, 0, st>>>(d_iter.get(), d_maxd.get());
             DRESS_CUDA_TRY(cudaGetLastError());
         }

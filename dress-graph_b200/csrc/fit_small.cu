@@ -3,11 +3,12 @@
 // Reference: libdress/src/dress.c:546-608 (the iteration driver) with the
 // vertex and edge phases of :556-591.  A graph whose whole fit state (edge
 // values twice, vertex norms) fits one SM's shared memory, with rows of at
-// most 31 neighbours, is fitted by one 512-thread CTA of the batch kernel as
+// most 256 neighbours, is fitted by one 512-thread CTA of the batch kernel as
 // a single whole-graph item: every sweep, the convergence test and the final
 // values in one launch, without per-sweep kernels or host round trips.  The
-// arithmetic is the batch kernel's, bit-identical to the reference's (sorted
-// Kahan-Babuska-Neumaier sums, separately rounded products).  The graph is
+// arithmetic is the batch kernel's, bit-identical to the reference's
+// (certified sums with the sorted Kahan-Babuska-Neumaier sum as their
+// fallback, separately rounded products).  The graph is
 // staged in shared memory as well.  Graphs of up to CLUSTER_MAX_EDGES edges
 // that do not fit one CTA run on a thread-block cluster instead, the state
 // spread over its CTAs' distributed shared memory (batch.cu,
@@ -30,13 +31,14 @@ constexpr int SMALL_GSIZE = 512;       // threads of the one group
 // the whole device (measured on G(n, m): 0.21-0.33 ms against 0.95 ms up to
 // 1500 edges, even at 3000, behind beyond).
 constexpr int SMALL_MAX_EDGES = 2048;
-// Beyond that, up to this many edges, one cluster of 8 CTAs holds the state
-// in its distributed shared memory and runs the fit in one launch.  Measured
-// on G(n, m) against the multi-kernel fit: 0.64 / 1.23 ms at 3000 edges,
-// 1.11 / 1.26 ms at 8000, 1.57 / 1.44 ms at 10000, 8.4 / 1.8 ms at 60000
-// (the per-thread load chains of eight SMs are latency-bound; clusters of 16
-// CTAs measured no better).
-constexpr int CLUSTER_MAX_EDGES = 8192;
+// Beyond that, up to this many edges, one cluster of 8 (or 16) CTAs holds
+// the state in its distributed shared memory and runs the fit in one
+// launch.  Measured per dress_fit_cuda call on G(n, m), one launch against
+// the multi-kernel fit: 0.39 / 1.10 ms at 3000 edges, 0.61 / 1.16 ms at
+// 8000, 0.70 / 1.19 ms at 10000, 0.87 / 1.23 ms at 15000, 1.10 / 1.27 ms at
+// 20000, 2.49 / 1.43 ms at 40000 (a cluster's per-thread load chains are
+// latency-bound, the multi-kernel fit pays about 1 ms of fixed cost).
+constexpr int CLUSTER_MAX_EDGES = 24576;
 // Rows up to this many neighbours: one thread sums an item's terms, so a
 // longer row would make one thread's serial loop the whole sweep; the
 // multi-kernel fit gives such rows a warp or a block.
@@ -214,34 +216,38 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         else return Status::Ok();
     }
 
-    // the packed parent: arrays of the graph, the pairs, the current values
-    std::vector<unsigned char> packed((size_t)PL.bytes, 0);
-    unsigned char *b = packed.data();
-    std::memcpy(b + PL.U, g->U, (size_t)E * 4);
-    std::memcpy(b + PL.V, g->V, (size_t)E * 4);
-    std::memcpy(b + PL.w, g->edge_weight, (size_t)E * 8);
-    std::memcpy(b + PL.row_off, g->adj_offset, (size_t)(N + 1) * 4);
-    if (S) std::memcpy(b + PL.row_eid, g->adj_edge_idx, (size_t)S * 4);
-    if (one_cta) {
-        std::memcpy(b + PL.ioff, ioff.data(), (size_t)(E + 1) * 4);
-        if (T) std::memcpy(b + PL.pairs, pairs.data(), (size_t)T * 8);
-    }
-    if (has_nw) std::memcpy(b + PL.nw, g->NW, (size_t)N * 8);
-    std::memcpy(b + PL.dinit, g->edge_dress, (size_t)E * 8);
-
+    // One device block holds everything: the packed parent image, the row
+    // targets (cluster: the device pair walk reads them), the descriptor, the
+    // chunk, the counter, the statistics and the results.  The host writes
+    // the inputs once, into the context's pinned stage, and one copy each
+    // way moves them.
+    auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t off_tgt = al((size_t)PL.bytes);
+    const size_t off_desc = al(off_tgt + (one_cta ? 0 : (size_t)S * sizeof(int)));
+    const size_t off_chunk = al(off_desc + sizeof(ParentDesc));
+    const size_t off_ctr = al(off_chunk + sizeof(Chunk));
+    const size_t off_stats = al(off_ctr + sizeof(int));
+    const size_t off_vals = al(off_stats + ST_WORDS * sizeof(unsigned long long));
+    const size_t total = off_vals + ((size_t)E + N) * sizeof(double);
     cudaStream_t st = ctx.st;
-    DevBuf<unsigned char> d_data;
-    DevBuf<double> d_values;
-    DevBuf<unsigned long long> d_stats;
-    DevBuf<ParentDesc> d_desc;
-    DevBuf<Chunk> d_chunk;
-    DevBuf<int> d_counter;
-    DRESS_TRY(d_data.alloc(packed.size(), st));
-    DRESS_TRY(d_values.alloc((size_t)E + N, st));
-    DRESS_TRY(d_stats.alloc(ST_WORDS, st));
-    DRESS_TRY(d_desc.alloc(1, st));
-    DRESS_TRY(d_chunk.alloc(1, st));
-    DRESS_TRY(d_counter.alloc(1, st));
+    DevBuf<unsigned char> d_blob;
+    DRESS_TRY(d_blob.alloc(total, st));
+    DRESS_TRY(ctx.stage->reserve(total));
+    unsigned char *h = (unsigned char *)ctx.stage->ptr();
+    unsigned char *dv = d_blob.get();
+    std::memcpy(h + PL.U, g->U, (size_t)E * 4);
+    std::memcpy(h + PL.V, g->V, (size_t)E * 4);
+    std::memcpy(h + PL.w, g->edge_weight, (size_t)E * 8);
+    std::memcpy(h + PL.row_off, g->adj_offset, (size_t)(N + 1) * 4);
+    if (S) std::memcpy(h + PL.row_eid, g->adj_edge_idx, (size_t)S * 4);
+    if (one_cta) {
+        std::memcpy(h + PL.ioff, ioff.data(), (size_t)(E + 1) * 4);
+        if (T) std::memcpy(h + PL.pairs, pairs.data(), (size_t)T * 8);
+    } else if (S) {
+        std::memcpy(h + off_tgt, g->adj_target, (size_t)S * 4);
+    }
+    if (has_nw) std::memcpy(h + PL.nw, g->NW, (size_t)N * 8);
+    std::memcpy(h + PL.dinit, g->edge_dress, (size_t)E * 8);
     ParentDesc P{};
     P.N = N;
     P.E = E;
@@ -255,18 +261,17 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     P.eps = epsilon;
     P.has_nw = has_nw;
     P.has_dinit = 1;
-    P.data = d_data.get();
-    P.values = d_values.get();
-    P.stats = d_stats.get();
+    P.data = dv;
+    P.values = (double *)(dv + off_vals);
+    P.stats = (unsigned long long *)(dv + off_stats);
     P.offset = 0;
     P.stride = 1;
     const Chunk ch{0, 1, 0};
-    DRESS_CUDA_TRY(counted_memcpy(d_data.get(), packed.data(), packed.size(), cudaMemcpyHostToDevice, st));
-    DevBuf<int> d_tgt;
+    std::memcpy(h + off_desc, &P, sizeof P);
+    std::memcpy(h + off_chunk, &ch, sizeof ch);
+    std::memset(h + off_ctr, 0, off_vals - off_ctr);           // counter and statistics
+    DRESS_CUDA_TRY(counted_memcpy(dv, h, off_vals, cudaMemcpyHostToDevice, st));
     if (!one_cta) {
-        DRESS_TRY(d_tgt.alloc((size_t)S, st));
-        DRESS_CUDA_TRY(counted_memcpy(d_tgt.get(), g->adj_target, (size_t)S * sizeof(int), cudaMemcpyHostToDevice, st));
-        unsigned char *dd = d_data.get();
         const size_t pair_smem = (size_t)(N + 1 + S) * sizeof(int);
         const int staged = pair_smem <= (size_t)smem_cap ? 1 : 0;
         static bool attr_set[64] = {};
@@ -275,18 +280,14 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
             attr_set[ctx.device] = true;
         }
         count_launch(), k_small_pairs<<<1, PAIR_THR, staged ? pair_smem : 0, st>>>(
-            N, E, (const int *)(dd + PL.row_off), d_tgt.get(), (const int *)(dd + PL.row_eid),
-            (const int *)(dd + PL.U), (const int *)(dd + PL.V), (int *)(dd + PL.ioff), (int2 *)(dd + PL.pairs), staged);
+            N, E, (const int *)(dv + PL.row_off), (const int *)(dv + off_tgt), (const int *)(dv + PL.row_eid),
+            (const int *)(dv + PL.U), (const int *)(dv + PL.V), (int *)(dv + PL.ioff), (int2 *)(dv + PL.pairs), staged);
         DRESS_CUDA_TRY(cudaGetLastError());
     }
-    DRESS_CUDA_TRY(counted_memcpy(d_desc.get(), &P, sizeof P, cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(counted_memcpy(d_chunk.get(), &ch, sizeof ch, cudaMemcpyHostToDevice, st));
-    DRESS_CUDA_TRY(cudaMemsetAsync(d_stats.get(), 0, ST_WORDS * sizeof(unsigned long long), st));
-    DRESS_CUDA_TRY(cudaMemsetAsync(d_counter.get(), 0, sizeof(int), st));
-    L.parents = d_desc.get();
-    L.chunks = d_chunk.get();
+    L.parents = (const ParentDesc *)(dv + off_desc);
+    L.chunks = (const Chunk *)(dv + off_chunk);
     L.nchunks = 1;
-    L.chunk_counter = d_counter.get();
+    L.chunk_counter = (int *)(dv + off_ctr);
 
     cudaEvent_t e0, e1;
     DRESS_CUDA_TRY(cudaEventCreate(&e0));
@@ -300,23 +301,20 @@ Status fit_small(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     if (one_cta) {
         DRESS_TRY(launch_batch(L, ctx.num_sms, st));
     } else {
-        Status ls = launch_cluster_fit(d_desc.get(), E, N, lnc, ctx.num_sms, st);
+        Status ls = launch_cluster_fit(L.parents, E, N, lnc, ctx.num_sms, st);
         if (ls.code == DRESSX_EUNSUPPORTED) return Status::Ok();     // the multi-kernel fit takes it
         DRESS_TRY(ls);
     }
     DRESS_CUDA_TRY(cudaEventRecord(e1, st));
 
-    unsigned long long sv[ST_WORDS];
-    DRESS_CUDA_TRY(counted_memcpy(sv, d_stats.get(), sizeof sv, cudaMemcpyDeviceToHost, st));
-    DRESS_CUDA_TRY(counted_memcpy(g->edge_dress, d_values.get(), (size_t)E * sizeof(double),
-                                   cudaMemcpyDeviceToHost, st));
+    // statistics and results come back in one copy through the stage
+    DRESS_CUDA_TRY(counted_memcpy(h + off_stats, dv + off_stats, total - off_stats, cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+    unsigned long long sv[ST_WORDS];
+    std::memcpy(sv, h + off_stats, sizeof sv);
+    std::memcpy(g->edge_dress, h + off_vals, (size_t)E * sizeof(double));
     // the norms of the last sweep (none without sweeps), as fit_graph leaves them
-    if (sv[ST_SWEEPS] > 0) {
-        DRESS_CUDA_TRY(counted_memcpy(g->vertex_dress, d_values.get() + E, (size_t)N * sizeof(double),
-                                       cudaMemcpyDeviceToHost, st));
-        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-    }
+    if (sv[ST_SWEEPS] > 0) std::memcpy(g->vertex_dress, h + off_vals + (size_t)E * sizeof(double), (size_t)N * sizeof(double));
     float it_ms = 0.f;
     cudaEventElapsedTime(&it_ms, e0, e1);
     if (iterations) *iterations = (int)(long long)sv[ST_ITERATIONS];

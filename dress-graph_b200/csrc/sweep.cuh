@@ -188,13 +188,16 @@ __global__ void __launch_bounds__(THR) k_vertex_thr(Sweep s, int begin, int end)
     }
 }
 
-// PAIRS false: the bin without common neighbours (the sum is the self term)
+// PAIRS false: the edges without common neighbours (the sum is the self
+// term).  Edge kernels take the items [begin, end) of `list` (edge ids), or
+// the edge ids [begin, end) themselves when list is null.
 template <bool UNIF, bool PAIRS>
-__global__ void __launch_bounds__(THR) k_edge_thr(Sweep s, int begin, int end)
+__global__ void __launch_bounds__(THR) k_edge_thr(Sweep s, const int *list, int begin, int end)
 {
     if (skipped(s)) return;
     double lmax = 0.0;
-    for (int j = begin + blockIdx.x * blockDim.x + threadIdx.x; j < end; j += gridDim.x * blockDim.x) {
+    for (int x = begin + blockIdx.x * blockDim.x + threadIdx.x; x < end; x += gridDim.x * blockDim.x) {
+        const int j = list ? list[x] : x;
         const int u = s.eu[j], v = s.ev[j];
         const double dj = s.d[j];
         const double self = self_term(s, u, v, own_prod<UNIF>(s, j, dj));
@@ -283,16 +286,17 @@ __global__ void __launch_bounds__(WARP_THR) k_vertex_grp(Sweep s, int begin, int
 }
 
 template <bool UNIF, int GW>
-__global__ void __launch_bounds__(WARP_THR) k_edge_grp(Sweep s, int begin, int end)
+__global__ void __launch_bounds__(WARP_THR) k_edge_grp(Sweep s, const int *list, int begin, int end)
 {
     if (skipped(s)) return;
     constexpr int IPW = 32 / GW;
     const int lane = threadIdx.x & (GW - 1);
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     double lmax = 0.0;
-    for (int j0 = begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * IPW; j0 < end; j0 += nwarps * IPW) {
-        const int j = j0 + (int)((threadIdx.x & 31) / GW);
-        const bool valid = j < end;
+    for (int x0 = begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * IPW; x0 < end; x0 += nwarps * IPW) {
+        const int x = x0 + (int)((threadIdx.x & 31) / GW);
+        const bool valid = x < end;
+        const int j = valid ? (list ? list[x] : x) : 0;
         long long pb = 0;
         int n = 0;
         if (valid) {
@@ -387,11 +391,12 @@ __global__ void __launch_bounds__(BLK_THR) k_vertex_blk(Sweep s, int begin, int 
 }
 
 template <bool UNIF>
-__global__ void __launch_bounds__(BLK_THR) k_edge_blk(Sweep s, int begin, int end)
+__global__ void __launch_bounds__(BLK_THR) k_edge_blk(Sweep s, const int *list, int begin, int end)
 {
     if (skipped(s)) return;
     double lmax = 0.0;
-    for (int j = begin + (int)blockIdx.x; j < end; j += gridDim.x) {
+    for (int x = begin + (int)blockIdx.x; x < end; x += gridDim.x) {
+        const int j = list ? list[x] : x;
         const long long pb = s.ioff[j];
         const int n = (int)(s.ioff[j + 1] - pb);
         const int2 *pp = s.pairs + pb;
@@ -526,63 +531,54 @@ Status set_sweep_attributes(size_t exact_smem)
     return Status::Ok();
 }
 
-// One phase: the block items on the side stream, beside the thread and warp
-// items on the main stream; then the exact sums of the queued items.
-template <bool UNIF, bool EDGE>
-Status launch_phase(const Sweep &s, const Bins &b, const LaunchCfg &c)
+// The edge items of a sweep: the edges without common neighbours are the
+// ids [0, e0); the others are listed by size class in `list`:
+// [cls[0], cls[1]) 1..16 pairs (a thread each), [cls[1], cls[2]) 257..512,
+// [cls[2], cls[3]) 65..256, [cls[3], cls[4]) 17..64 (lane groups of 32, 16,
+// 8), [cls[4], cls[5]) 513..BIG_CAP (a warp each), [cls[5], cls[6]) more (a
+// block each).
+struct EdgeClasses {
+    int e0;
+    const int *list;
+    int cls[7];
+};
+
+template <bool UNIF>
+void launch_grp(const Sweep &s, const int *list, int lo, int hi, int gw, const LaunchCfg &c, bool edge)
 {
-    // items beyond BIG_CAP terms: a block each, on the side stream
+    if (hi <= lo) return;
+    const unsigned g = grid_for((long long)(hi - lo) * gw, WARP_THR, 16LL * c.sms);
+    count_launch();
+    switch (gw) {
+    case 32: edge ? k_edge_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, list, lo, hi)
+                  : k_vertex_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, lo, hi); break;
+    case 16: edge ? k_edge_grp<UNIF, 16><<<g, WARP_THR, 0, c.st>>>(s, list, lo, hi)
+                  : k_vertex_grp<UNIF, 16><<<g, WARP_THR, 0, c.st>>>(s, lo, hi); break;
+    default: edge ? k_edge_grp<UNIF, 8><<<g, WARP_THR, 0, c.st>>>(s, list, lo, hi)
+                  : k_vertex_grp<UNIF, 8><<<g, WARP_THR, 0, c.st>>>(s, lo, hi); break;
+    }
+}
+
+// Vertex phase: rows beyond BIG_CAP slots a block each on the side stream,
+// beside the warp and thread rows on the main stream; then the exact sums
+// of the queued rows.
+template <bool UNIF>
+Status launch_vertex_phase(const Sweep &s, const Bins &b, const LaunchCfg &c)
+{
     const bool blocks = b.has(BBIG);
     if (blocks) {
         DRESS_CUDA_TRY(cudaEventRecord(c.fork, c.st));
         DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
         const int lo = b.start[BBIG], hi = b.start[BBIG + 1];
-        const unsigned g = grid_for(hi - lo, 1, 8LL * c.sms);
-        count_launch();
-        if (EDGE) k_edge_blk<UNIF><<<g, BLK_THR, 0, c.side>>>(s, lo, hi);
-        else k_vertex_blk<UNIF><<<g, BLK_THR, 0, c.side>>>(s, lo, hi);
+        count_launch(), k_vertex_blk<UNIF><<<grid_for(hi - lo, 1, 8LL * c.sms), BLK_THR, 0, c.side>>>(s, lo, hi);
     }
-    // MED_CAP..BIG_CAP terms: a warp each (16 to 128 terms a lane)
-    if (b.has(BBLOCK)) {
-        const int lo = b.start[BBLOCK], hi = b.start[BBLOCK + 1];
-        const unsigned g = grid_for((long long)(hi - lo) * 32, WARP_THR, 16LL * c.sms);
-        count_launch();
-        if (EDGE) k_edge_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, lo, hi);
-        else k_vertex_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, lo, hi);
-    }
+    launch_grp<UNIF>(s, nullptr, b.start[BBLOCK], b.start[BBLOCK + 1], 32, c, false);
     if (b.has(BMED)) {
-        // [med[0], med[1]): more than 256 terms, [med[1], med[2]): 65..256,
-        // [med[2], med[3]): 17..64 (the bin is ordered longest first)
-        const int *m = b.med;
-        if (m[1] > m[0]) {
-            const unsigned g = grid_for((long long)(m[1] - m[0]) * 32, WARP_THR, 16LL * c.sms);
-            count_launch();
-            if (EDGE) k_edge_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, m[0], m[1]);
-            else k_vertex_grp<UNIF, 32><<<g, WARP_THR, 0, c.st>>>(s, m[0], m[1]);
-        }
-        if (m[2] > m[1]) {
-            const unsigned g = grid_for((long long)(m[2] - m[1]) * 16, WARP_THR, 16LL * c.sms);
-            count_launch();
-            if (EDGE) k_edge_grp<UNIF, 16><<<g, WARP_THR, 0, c.st>>>(s, m[1], m[2]);
-            else k_vertex_grp<UNIF, 16><<<g, WARP_THR, 0, c.st>>>(s, m[1], m[2]);
-        }
-        if (m[3] > m[2]) {
-            const unsigned g = grid_for((long long)(m[3] - m[2]) * 8, WARP_THR, 16LL * c.sms);
-            count_launch();
-            if (EDGE) k_edge_grp<UNIF, 8><<<g, WARP_THR, 0, c.st>>>(s, m[2], m[3]);
-            else k_vertex_grp<UNIF, 8><<<g, WARP_THR, 0, c.st>>>(s, m[2], m[3]);
-        }
+        launch_grp<UNIF>(s, nullptr, b.med[0], b.med[1], 32, c, false);
+        launch_grp<UNIF>(s, nullptr, b.med[1], b.med[2], 16, c, false);
+        launch_grp<UNIF>(s, nullptr, b.med[2], b.med[3], 8, c, false);
     }
-    if (EDGE) {
-        // edges without common neighbours, then the thread bins with pairs
-        if (b.has(B0)) {
-            count_launch(), k_edge_thr<UNIF, false><<<grid_for(b.count(B0), THR, 16LL * c.sms), THR, 0, c.st>>>(
-                s, b.start[B0], b.start[B0 + 1]);
-        }
-        const int lo = b.start[B2], hi = b.start[BMED];
-        if (hi > lo)
-            count_launch(), k_edge_thr<UNIF, true><<<grid_for(hi - lo, THR, 16LL * c.sms), THR, 0, c.st>>>(s, lo, hi);
-    } else {
+    {
         const int lo = b.start[B0], hi = b.start[BMED];
         if (hi > lo)
             count_launch(), k_vertex_thr<UNIF><<<grid_for(hi - lo, THR, 16LL * c.sms), THR, 0, c.st>>>(s, lo, hi);
@@ -591,17 +587,46 @@ Status launch_phase(const Sweep &s, const Bins &b, const LaunchCfg &c)
         DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
         DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
     }
-    count_launch();
-    if (EDGE) k_edge_exact<UNIF><<<c.exact_grid, EXACT_THR, c.exact_smem, c.st>>>(s);
-    else k_vertex_exact<UNIF><<<c.exact_grid, EXACT_THR, c.exact_smem, c.st>>>(s);
+    count_launch(), k_vertex_exact<UNIF><<<c.exact_grid, EXACT_THR, c.exact_smem, c.st>>>(s);
+    return Status::Ok();
+}
+
+// Edge phase: the same shape over the edge classes.
+template <bool UNIF>
+Status launch_edge_phase(const Sweep &s, const EdgeClasses &ec, const LaunchCfg &c)
+{
+    const int *L = ec.list;
+    const int *k = ec.cls;
+    const bool blocks = k[6] > k[5];
+    if (blocks) {
+        DRESS_CUDA_TRY(cudaEventRecord(c.fork, c.st));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.side, c.fork, 0));
+        count_launch(), k_edge_blk<UNIF><<<grid_for(k[6] - k[5], 1, 8LL * c.sms), BLK_THR, 0, c.side>>>(
+            s, L, k[5], k[6]);
+    }
+    launch_grp<UNIF>(s, L, k[4], k[5], 32, c, true);
+    launch_grp<UNIF>(s, L, k[1], k[2], 32, c, true);
+    launch_grp<UNIF>(s, L, k[2], k[3], 16, c, true);
+    launch_grp<UNIF>(s, L, k[3], k[4], 8, c, true);
+    if (ec.e0 > 0)
+        count_launch(), k_edge_thr<UNIF, false><<<grid_for(ec.e0, THR, 16LL * c.sms), THR, 0, c.st>>>(
+            s, nullptr, 0, ec.e0);
+    if (k[1] > k[0])
+        count_launch(), k_edge_thr<UNIF, true><<<grid_for(k[1] - k[0], THR, 16LL * c.sms), THR, 0, c.st>>>(
+            s, L, k[0], k[1]);
+    if (blocks) {
+        DRESS_CUDA_TRY(cudaEventRecord(c.join, c.side));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(c.st, c.join, 0));
+    }
+    count_launch(), k_edge_exact<UNIF><<<c.exact_grid, EXACT_THR, c.exact_smem, c.st>>>(s);
     return Status::Ok();
 }
 
 template <bool UNIF>
-Status launch_sweep(const Sweep &s, const Bins &vb, const Bins &eb, const LaunchCfg &c)
+Status launch_sweep(const Sweep &s, const Bins &vb, const EdgeClasses &ec, const LaunchCfg &c)
 {
-    DRESS_TRY((launch_phase<UNIF, false>(s, vb, c)));
-    DRESS_TRY((launch_phase<UNIF, true>(s, eb, c)));
+    DRESS_TRY(launch_vertex_phase<UNIF>(s, vb, c));
+    DRESS_TRY(launch_edge_phase<UNIF>(s, ec, c));
     count_launch(), k_clear_queues<<<1, 1, 0, c.st>>>(s.qcount);
     DRESS_CUDA_TRY(cudaGetLastError());
     return Status::Ok();

@@ -285,3 +285,27 @@ def test_device_graph_build_rejects_bad_ids_and_fits_alike(oracle_port):
     ref = oracle_port.fit(n, U, V)
     assert it == ref["iterations"]
     np.testing.assert_array_equal(bits(ed), bits(ref["edge_dress"]))
+
+
+def test_large_fit_digests():
+    """The single-fit workload at full size -- Chung-Lu, 4M vertices, 28M
+    edges, weighted U[0.5, 2] and unweighted -- against the reference's own
+    dress_fit_omp on the same graph: identical iteration count, final delta
+    and SHA-256 digests of every edge and vertex value
+    (tests/golden/large_fit.json, made by tests/golden/make_large_golden.py)."""
+    import hashlib
+    with open(os.path.join(ROOT, "tests", "golden", "large_fit.json")) as f:
+        gold = json.load(f)
+    sha = lambda a: hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+    n, U, V = graphs.chung_lu(4_000_000, 28_000_000, 2.3, 20000, seed=42)
+    W = graphs.uniform_weights(len(U), seed=7)
+    assert (n, len(U)) == (gold["graph"]["N"], gold["graph"]["E"])
+    assert sha(U) == gold["graph"]["sha_U"] and sha(V) == gold["graph"]["sha_V"] and sha(W) == gold["graph"]["sha_W"]
+    for label, w in (("weighted", W), ("unweighted", None)):
+        ref = gold[label]["full"]
+        with db.Graph(n, U, V, w, device_build=True) as g:
+            it, dl = db.fit_graph(g, 100, 1e-6)
+            assert it == ref["iterations"], label
+            assert int(np.float64(dl).view(np.int64)) == ref["delta_bits"], label
+            assert sha(g.edge_dress) == ref["sha_edge_dress"], label
+            assert sha(g.vertex_dress) == ref["sha_vertex_dress"], label
