@@ -127,6 +127,12 @@ struct Group {
         if (size == 32) __syncwarp();
         else asm volatile("bar.sync %0, %1;" ::"r"(gid + 1), "r"(size) : "memory");
     }
+    // after group_max: a group wider than a warp has just passed a barrier
+    // there; a warp's shuffles order no shared-memory writes
+    __device__ __forceinline__ void sync_after_reduce() const
+    {
+        if (size == 32) __syncwarp();
+    }
 };
 
 // The masked subgraph of one item: deleted (Delta) or marked (Nabla) vertices.
@@ -191,6 +197,8 @@ struct ClusterGroup {
     double *const *part;         // every CTA's two partial slots
     int ncta;
     __device__ __forceinline__ void sync() const { cg::this_cluster().sync(); }
+    // after group_max: every thread has just passed its cluster barrier
+    __device__ __forceinline__ void sync_after_reduce() const {}
 };
 
 struct DArr {
@@ -367,7 +375,10 @@ __device__ void fit_item(const ParentDesc &P, const View &G, long long item,
         const Arr t = d0;
         d0 = d1;
         d1 = t;
-        g.sync();
+        // The reduction's barrier already orders this sweep's writes of d1
+        // and its reads of vd and d0 before the next sweep's writes; its
+        // slots alternate by parity.
+        g.sync_after_reduce();
         if (m < P.eps) break;
     }
     const int sweeps = it < P.max_iter ? it + 1 : P.max_iter;

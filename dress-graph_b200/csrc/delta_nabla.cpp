@@ -738,6 +738,7 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
     double best_rate = 0.0;
     Status err;
     Tune best_tu{0, 0, 1};
+    std::vector<std::pair<double, Tune>> tried;
     for (const Cand &cd : cands) {
         const int gs = cd.gs;
         Tune tu{gs, gs == 32 ? 16 : std::min(15, 512 / gs), cd.per_sm};
@@ -762,8 +763,8 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
         L.chunks = d_try.get();
         L.nchunks = (int)ch.size();
         float ms = 0.f;
-        float best_ms = 0.f;
-        for (int rep = 0; rep < 3; ++rep) {          // the first run is untimed; the faster of two
+        std::vector<float> times;
+        for (int rep = 0; rep < 4; ++rep) {          // the first run is untimed; the median of three
             cudaMemsetAsync(P.d_stats.get(), 0, ST_WORDS * P.ps.size() * sizeof(unsigned long long), st);
             cudaMemsetAsync(P.d_counter.get(), 0, sizeof(int), st);
             cudaEventRecord(e0, st);
@@ -775,17 +776,25 @@ Status autotune_batched(BatchPlan &P, const Ctx &en, int *best_out, std::vector<
                 break;
             }
             cudaEventElapsedTime(&ms, e0, e1);
-            if (rep == 1 || (rep > 1 && ms < best_ms)) best_ms = ms;
+            if (rep > 0) times.push_back(ms);
         }
         if (!err.ok()) break;
-        const double rate = best_ms > 0.f ? (double)items / best_ms : 0.0;
+        std::sort(times.begin(), times.end());
+        const float med = times.empty() ? 0.f : times[times.size() / 2];
+        const double rate = med > 0.f ? (double)items / med : 0.0;
         if (rates) rates->push_back((float)rate);
-        if (rate > best_rate) {
-            best_rate = rate;
-            best = gs;
-            best_tu = tu;
-        }
+        tried.push_back({rate, tu});
+        best_rate = std::max(best_rate, rate);
     }
+    // The first candidate, in the fixed order above, within 3 % of the
+    // fastest: schedules that differ by less than the run-to-run noise then
+    // resolve the same way on every run.
+    for (const auto &t : tried)
+        if (t.first > 0.0 && t.first >= 0.97 * best_rate) {
+            best = t.second.gsize;
+            best_tu = t.second;
+            break;
+        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     DRESS_TRY(err);

@@ -119,15 +119,17 @@ typedef struct dressx_batch dressx_batch_t;
 int  dressx_batch_create(dressx_hist_request_t *reqs, int n, dressx_batch_t **out);
 /* All fits and histograms on the device; results stay in device memory. */
 int  dressx_batch_run(dressx_batch_t *b);
-/* Autotuner: runs the batch kernel on a sample of this batch's subgraphs
- * with 32, 64, 128 and 256 threads per subgraph, one 512-thread CTA per SM,
- * and (networks of at most 16 terms) with 32, 64 and 128 threads per
- * subgraph and two CTAs sharing each SM -- each schedule where one subgraph's
- * state fits shared memory -- keeps the fastest for the batch's size class
- * (batches of that class planned later in the process start from it) and
- * re-plans this batch with it.  *group_threads and *ctas_per_sm (nullable)
- * get the winner; rates[8] (nullable) the sampled subgraph-fits per ms of
- * the candidates in that order (0 = did not fit). */
+/* Autotuner: runs the batch kernel on this batch's subgraphs (a spread
+ * sample beyond 200K) with 32, 64, 128 and 256 threads per subgraph and one
+ * 512-thread CTA per SM, then 32, 64 and 128 threads with two CTAs sharing
+ * each SM -- each schedule where one subgraph's state fits shared memory --
+ * timing the median of three runs after an untimed one.  It keeps the first
+ * schedule, in that order, within 3 % of the fastest (so schedules closer
+ * than the run-to-run noise resolve the same way every time) for the
+ * batch's size class (batches of that class planned later in the process
+ * start from it) and re-plans this batch with it.  *group_threads and
+ * *ctas_per_sm (nullable) get the winner; rates[8] (nullable) the
+ * subgraph-fits per ms of the candidates in that order (0 = did not fit). */
 int  dressx_batch_autotune(dressx_batch_t *b, int *group_threads, int *ctas_per_sm, float *rates);
 /* Captures the fit stage (counter resets and the batch kernel) into a CUDA
  * graph; later dressx_batch_run calls replay it with one launch. */

@@ -190,7 +190,10 @@ def test_autotuned_and_captured_batch_matches(kind, k):
     b = db.Batch(objs, kind, k)
     best, per_sm, rates = b.autotune()
     assert best in (32, 64, 128, 256) and per_sm in (1, 2)
-    assert rates[(best, per_sm)] == max(rates.values()) > 0
+    # the first schedule, in the fixed candidate order, within 3 % of the fastest
+    top = max(rates.values())
+    assert top > 0 and rates[(best, per_sm)] >= 0.97 * top
+    assert next(k for k, r in rates.items() if r >= 0.97 * top) == (best, per_sm)
     b.run()
     for x, y in zip(b.fetch(), expect):
         np.testing.assert_array_equal(x, y)
