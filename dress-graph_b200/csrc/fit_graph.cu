@@ -367,6 +367,109 @@ __global__ void k_new_rows(int N, const int *vperm, const int *off, const int *e
     }
 }
 
+// ---- the second copy of the products (large simple undirected graphs) ----
+// Every edge with common neighbours has an owner (the endpoint of lower
+// (degree, id) rank) and a non-owner.  Its product lives at its id, in the
+// owner's runs; the vertex phase also writes it, as it gathers it anyway,
+// into a copy area Q after the E products, at qpos[e], inside the
+// non-owner's contiguous run [qbeg[v], qbeg[v+1]).  The common-neighbour
+// pair (e_ux, e_vx) of edge (u, v) then refers to e_ux in u's data -- its
+// id if u owns it, E + qpos[e_ux] if not -- and to e_vx in v's data, so the
+// gathers of an edge fall into four contiguous runs instead of scattering
+// over the array.
+
+// owner of every edge, in the new numbering of edges and vertices
+__global__ void k_edge_owner(int E, const int *eperm, const int *U, const int *V, const int *deg, const int *vinv,
+                             int *own)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
+        const int e = eperm[j], u = U[e], v = V[e];
+        own[j] = vinv[rank_key(deg, u) <= rank_key(deg, v) ? u : v];
+    }
+}
+
+// slot class of new vertex i's slot with new edge id en: 0 owned by i,
+// 1 not owned and with common neighbours (ids from e0 on), 2 the rest
+__device__ __forceinline__ int slot_class(int en, int i, const int *own, int e0)
+{
+    return own[en] == i ? 0 : en >= e0 ? 1 : 2;
+}
+
+// per new vertex: its slots of class 1 (one warp per vertex)
+__global__ void k_q_count(int N, const int *vperm, const int *off, const int *eidx, const int *einv, const int *own,
+                          int e0, int *nq)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        const int u = vperm[i], b = off[u], n = off[u + 1] - b;
+        int c = 0;
+        for (int k = lane; k < n; k += 32) c += slot_class(einv[eidx[b + k]], i, own, e0) == 1;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) nq[i] = c;
+    }
+}
+
+// the new rows, each stably partitioned into its class 0, 1, 2 slots; the
+// class-1 slots get their copy positions, rq[i] is where they start in the row
+__global__ void k_new_rows_q(int N, const int *vperm, const int *off, const int *eidx, const int *einv,
+                             const int *own, int e0, const long long *row_off, const long long *qbeg, int *row_eid,
+                             int *qpos, int *rq, const double *nw_in, double *nw_out)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    unsigned lt;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
+        const int u = vperm[i], b = off[u], n = off[u + 1] - b;
+        int n0 = 0;
+        for (int k = lane; k < n; k += 32) n0 += slot_class(einv[eidx[b + k]], i, own, e0) == 0;
+        for (int o = 16; o > 0; o >>= 1) n0 += __shfl_xor_sync(0xffffffffu, n0, o);
+        const int n1 = (int)(qbeg[i + 1] - qbeg[i]);
+        int at[3] = {0, n0, n0 + n1};
+        const long long o = row_off[i];
+        for (int k0 = 0; k0 < n; k0 += 32) {
+            const int k = k0 + lane;
+            const int en = k < n ? einv[eidx[b + k]] : -1;
+            const int c = k < n ? slot_class(en, i, own, e0) : 3;
+            const unsigned m0 = __ballot_sync(0xffffffffu, c == 0), m1 = __ballot_sync(0xffffffffu, c == 1),
+                           m2 = __ballot_sync(0xffffffffu, c == 2);
+            if (c < 3) {
+                const unsigned m = c == 0 ? m0 : c == 1 ? m1 : m2;
+                const int pos = at[c] + __popc(m & lt);
+                row_eid[o + pos] = en;
+                if (c == 1) qpos[en] = (int)qbeg[i] + (pos - n0);
+            }
+            at[0] += __popc(m0);
+            at[1] += __popc(m1);
+            at[2] += __popc(m2);
+        }
+        if (lane == 0) {
+            rq[i] = n0;
+            nw_out[i] = nw_in[u];
+        }
+    }
+}
+
+// the pairs of every edge as references into the products and their copy:
+// the side sharing u (v) read from u's (v's) data
+__global__ void k_pair_refs(int E, const long long *ioff, const int *eu, const int *ev, const int *own,
+                            const int *qpos, int2 *pairs)
+{
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
+        const int u = eu[j], v = ev[j];
+        const long long b = ioff[j], n = ioff[j + 1] - b;
+        for (long long k = 0; k < n; ++k) {
+            const int2 pr = pairs[b + k];
+            const bool xu = eu[pr.x] == u || ev[pr.x] == u;
+            const int au = xu ? pr.x : pr.y, av = xu ? pr.y : pr.x;
+            const int ru = own[au] == u ? au : E + qpos[au];
+            const int rv = own[av] == v ? av : E + qpos[av];
+            pairs[b + k] = make_int2(ru, rv);
+        }
+    }
+}
+
 __global__ void k_new_edges(int E, const int *eperm, const int *U, const int *V, const int *vinv,
                             const double *w, const double *d, const int *cnt, int *eu, int *ev,
                             double *wn, double *d0, double *p0, int *ncnt)
@@ -667,19 +770,52 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_nwi.alloc((size_t)N, st));
     count_launch(), k_gather_deg<<<vg, 256, 0, st>>>(N, d_vperm.get(), d_deg.get(), d_ndeg.get());
     DRESS_TRY(exclusive_scan_i32(d_ndeg.get(), d_row_off.get(), N, d_scan_tmp.get(), st));
-    count_launch(), k_new_rows<<<grid_for((long long)N * 32, 256, 64 * sms), 256, 0, st>>>(
-        N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(), d_row_off.get(), d_row_eid.get(),
-        d_nw.get(), d_nwi.get());
+    // The second copy of the products (see k_pair_refs): large simple
+    // undirected graphs, whose pairs come from the triangle listing.
+    const bool qmode = locality && !(g->precompute_intercepts && g->intercept_offset) &&
+                       g->variant == DRESS_VARIANT_UNDIRECTED && !dup && E - eb.count(B0) > 0;
+    DevBuf<int> d_own, d_qpos, d_rq, d_nq;
+    DevBuf<long long> d_qbeg;
+    long long Qn = 0;
+    if (qmode) {
+        const int e0q = eb.count(B0);
+        DRESS_TRY(d_own.alloc((size_t)E, st));
+        DRESS_TRY(d_qpos.alloc((size_t)E, st));
+        DRESS_TRY(d_rq.alloc((size_t)N, st));
+        DRESS_TRY(d_nq.alloc((size_t)N, st));
+        DRESS_TRY(d_qbeg.alloc((size_t)N + 1, st));
+        count_launch(), k_edge_owner<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_U.get(), d_V.get(), d_deg.get(),
+                                                         d_vinv.get(), d_own.get());
+        const unsigned wg = grid_for((long long)N * 32, 256, 64 * sms);
+        count_launch(), k_q_count<<<wg, 256, 0, st>>>(N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(),
+                                                      d_own.get(), e0q, d_nq.get());
+        DRESS_TRY(exclusive_scan_i32(d_nq.get(), d_qbeg.get(), N, d_scan_tmp.get(), st));
+        count_launch(), k_new_rows_q<<<wg, 256, 0, st>>>(N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(),
+                                                         d_own.get(), e0q, d_row_off.get(), d_qbeg.get(),
+                                                         d_row_eid.get(), d_qpos.get(), d_rq.get(), d_nw.get(),
+                                                         d_nwi.get());
+        DRESS_CUDA_TRY(counted_memcpy(&Qn, d_qbeg.get() + N, sizeof(Qn), cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+        d_nq.release();
+    } else {
+        count_launch(), k_new_rows<<<grid_for((long long)N * 32, 256, 64 * sms), 256, 0, st>>>(
+            N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(), d_row_off.get(), d_row_eid.get(),
+            d_nw.get(), d_nwi.get());
+    }
     d_eidx.release();
     d_ndeg.release();
+    // value and product buffers: E entries, then the copy area (uniform
+    // weights gather the values, other graphs the products)
+    const size_t dstride = (size_t)E + (uniform ? (size_t)Qn : 0);
+    const size_t pstride = (size_t)E + (size_t)Qn;
 
     DRESS_TRY(d_eu.alloc((size_t)E, st));
     DRESS_TRY(d_ev.alloc((size_t)E, st));
     DRESS_TRY(d_ncnt.alloc((size_t)E, st));
-    DRESS_TRY(d_dbuf.alloc(2 * (size_t)E, st));
+    DRESS_TRY(d_dbuf.alloc(2 * dstride, st));
     if (!uniform) {
         DRESS_TRY(d_wi.alloc((size_t)E, st));
-        DRESS_TRY(d_pbuf.alloc(2 * (size_t)E, st));
+        DRESS_TRY(d_pbuf.alloc(2 * pstride, st));
     }
     count_launch(), k_new_edges<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_U.get(), d_V.get(), d_vinv.get(), d_w.get(),
                                     d_d.get(), d_cnt.get(), d_eu.get(), d_ev.get(),
@@ -732,6 +868,12 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_pairs.alloc((size_t)(T > 0 ? T : 1), st));
     count_launch(), k_new_pairs<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_ioff_old.get(), d_pairs_old.get(), d_einv.get(),
                                     d_ioff.get(), d_pairs.get());
+    if (qmode) {
+        count_launch(), k_pair_refs<<<eg, 256, 0, st>>>(E, d_ioff.get(), d_eu.get(), d_ev.get(), d_own.get(),
+                                                        d_qpos.get(), d_pairs.get());
+        d_own.release();
+        d_qpos.release();
+    }
     DRESS_CUDA_TRY(cudaGetLastError());
     d_pairs_old.release();
     // each edge's pairs in e_ux order: a warp's lanes then gather neighbouring
@@ -804,8 +946,11 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_CUDA_TRY(cudaMemsetAsync(d_qcount.get(), 0, 2 * sizeof(unsigned), st));
     s.qv = d_qv.get(); s.qe = d_qe.get(); s.qcount = d_qcount.get();
     LaunchCfg lc{sms, exact_grid, exact_smem, st, ctx.side, ctx.fork, ctx.join};
-    double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + E};
-    double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + E};
+    double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + dstride};
+    double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + pstride};
+    s.qbeg = qmode ? d_qbeg.get() : nullptr;
+    s.qw = nullptr;
+    s.rq = qmode ? d_rq.get() : nullptr;
 
     // Two sweeps (the even one writes buffer 1, the odd one buffer 0) and the
     // index steps between them are captured once into a CUDA graph, replayed
@@ -820,6 +965,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     for (int par = 0; par < 2; ++par) {
         sw2[par].d = dbuf[par]; sw2[par].dn = dbuf[par ^ 1];
         sw2[par].p = pbuf[par]; sw2[par].pn = pbuf[par ^ 1];
+        sw2[par].qw = qmode ? (uniform ? dbuf[par] : pbuf[par]) + E : nullptr;
     }
     auto enqueue_pair = [&]() -> Status {
         for (int par = 0; par < 2; ++par) {

@@ -79,3 +79,10 @@ def test_batched_delta_nabla_sorted_path(oracle_port, exact_sums):
             np.testing.assert_array_equal(flat, fn(n, U, V, k=1)["hist"])
     for g in objs:
         g.close()
+
+
+def test_large_graph_layout_sorted_path(oracle_port, exact_sums):
+    # the renumbered layout of a graph above 2^20 edges, every item sorted
+    n, U, V = graphs.chung_lu(200_000, 1_200_000, 2.3, 3000, seed=5)
+    W = graphs.uniform_weights(len(U), seed=6)
+    assert_same(gpu_fit(n, U, V, W, max_iterations=4), oracle_port.fit(n, U, V, W, precompute=1, max_iterations=4))

@@ -309,3 +309,15 @@ def test_large_fit_digests():
             assert int(np.float64(dl).view(np.int64)) == ref["delta_bits"], label
             assert sha(g.edge_dress) == ref["sha_edge_dress"], label
             assert sha(g.vertex_dress) == ref["sha_vertex_dress"], label
+
+
+def test_large_graph_layout(oracle_port):
+    """A power-law graph above the size where the fit renumbers edges for
+    gather locality (2^20 edges): owner order, per-class edge lists and the
+    product copy that the vertex phase writes for the pair gathers --
+    weighted with vertex weights, and unweighted -- against the oracle."""
+    n, U, V = graphs.chung_lu(200_000, 1_200_000, 2.3, 3000, seed=5)
+    W = graphs.uniform_weights(len(U), seed=6)
+    NW = np.random.default_rng(3).uniform(0.5, 2.0, n)
+    assert_same(gpu_fit(n, U, V, W, NW, max_iterations=30), oracle_port.fit(n, U, V, W, NW, precompute=1, max_iterations=30))
+    assert_same(gpu_fit(n, U, V, max_iterations=30), oracle_port.fit(n, U, V, precompute=1, max_iterations=30))
