@@ -661,10 +661,11 @@ def bench_serving(args, clocks):
            "total_edges": int(sum(g.E for g in objs)), "rates": []}
     clocks.start()
     with db.Server() as srv:
-        # warm-up pass over the first requests (kernel attributes, arena growth)
-        for g in objs[:20]:
+        # untimed warm-up pass over the whole stream, submitted at once: kernel
+        # attributes, and the arena grown to the stream's peak before any rate
+        for g in objs:
             _reset_edges(g)
-        ws = [srv.submit(g, k, 1 if k == 0 else 0) for g, k in zip(objs[:20], kinds[:20])]
+        ws = [srv.submit(g, k, 1 if k == 0 else 0) for g, k in zip(objs, kinds)]
         srv.drain()
         assert all(t.result()["status"] == 0 for t in ws)
         for rate in [float(x) for x in args.serve_rates.split(",") if x]:

@@ -95,23 +95,23 @@ void host_part(const HostSpan *spans, int n, char *stage, size_t k, size_t total
     });
 }
 
-Status staged_copy(const HostSpan *spans, int n, const Ctx &ctx, bool up)
+Status staged_copy(const HostSpan *spans, int n, Pinned *pin, cudaStream_t cs, bool up)
 {
     size_t total = 0;
     for (int i = 0; i < n; ++i) total += spans[i].bytes;
     if (total == 0) return Status::Ok();
-    if (total <= ((size_t)1 << 20) || !ctx.stage) {
+    if (total <= ((size_t)1 << 20) || !pin) {
         // small copies: the driver's own staging is as quick
         for (int i = 0; i < n; ++i) {
             if (!spans[i].bytes) continue;
-            if (up) DRESS_CUDA_TRY(counted_memcpy(spans[i].dev, spans[i].host, spans[i].bytes, cudaMemcpyHostToDevice, ctx.st));
-            else DRESS_CUDA_TRY(counted_memcpy(spans[i].host, spans[i].dev, spans[i].bytes, cudaMemcpyDeviceToHost, ctx.st));
+            if (up) DRESS_CUDA_TRY(counted_memcpy(spans[i].dev, spans[i].host, spans[i].bytes, cudaMemcpyHostToDevice, cs));
+            else DRESS_CUDA_TRY(counted_memcpy(spans[i].host, spans[i].dev, spans[i].bytes, cudaMemcpyDeviceToHost, cs));
         }
-        DRESS_CUDA_TRY(cudaStreamSynchronize(ctx.st));
+        DRESS_CUDA_TRY(cudaStreamSynchronize(cs));
         return Status::Ok();
     }
-    DRESS_TRY(ctx.stage->reserve(2 * STAGE_CHUNK));
-    char *stage = ctx.stage->ptr();
+    DRESS_TRY(pin->reserve(2 * STAGE_CHUNK));
+    char *stage = pin->ptr();
     cudaEvent_t ev[2] = {nullptr, nullptr};
     for (auto &e : ev) DRESS_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     struct EvGuard {
@@ -132,15 +132,15 @@ Status staged_copy(const HostSpan *spans, int n, const Ctx &ctx, bool up)
         if (up) host_part(spans, n, stage, k, total, true);
         Status err;
         for_pieces(spans, n, lo, hi, [&](const HostSpan &sp, size_t off, size_t len, size_t at) {
-            cudaError_t e = up ? cudaMemcpyAsync((char *)sp.dev + off, slot + at, len, cudaMemcpyHostToDevice, ctx.st)
+            cudaError_t e = up ? cudaMemcpyAsync((char *)sp.dev + off, slot + at, len, cudaMemcpyHostToDevice, cs)
                                : cudaMemcpyAsync(slot + at, (const char *)sp.dev + off, len, cudaMemcpyDeviceToHost,
-                                                 ctx.st);
+                                                 cs);
             if (e != cudaSuccess && err.ok()) err = Status::Err(DRESSX_ECUDA, cudaGetErrorString(e));
         });
         DRESS_TRY(err);
         if (up) count_h2d(hi - lo);
         else count_d2h(hi - lo);
-        DRESS_CUDA_TRY(cudaEventRecord(ev[k & 1], ctx.st));
+        DRESS_CUDA_TRY(cudaEventRecord(ev[k & 1], cs));
         if (!up && k >= 1) {
             // the previous chunk is on the host: copy it out while this one is in flight
             DRESS_CUDA_TRY(cudaEventSynchronize(ev[(k - 1) & 1]));
@@ -156,8 +156,18 @@ Status staged_copy(const HostSpan *spans, int n, const Ctx &ctx, bool up)
 
 }  // namespace
 
-Status staged_upload(const HostSpan *spans, int n, const Ctx &ctx) { return staged_copy(spans, n, ctx, true); }
-Status staged_download(const HostSpan *spans, int n, const Ctx &ctx) { return staged_copy(spans, n, ctx, false); }
+Status staged_upload(const HostSpan *spans, int n, const Ctx &ctx)
+{
+    return staged_copy(spans, n, ctx.stage, ctx.st, true);
+}
+Status staged_download(const HostSpan *spans, int n, const Ctx &ctx)
+{
+    return staged_copy(spans, n, ctx.stage, ctx.st, false);
+}
+Status staged_upload_via(const HostSpan *spans, int n, Pinned *stage, cudaStream_t st)
+{
+    return staged_copy(spans, n, stage, st, true);
+}
 
 thread_local cudaMemPool_t tls_pool = nullptr;
 thread_local long long tls_launches = 0;
@@ -176,6 +186,7 @@ Status Ctx::create(int dev, int sms, const dressx_config_t *config, int priority
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join2, cudaEventDisableTiming));
     DRESS_CUDA_TRY(cudaEventCreateWithFlags(&join3, cudaEventDisableTiming));
     stage = new Pinned();
+    stage2 = new Pinned();
     return Status::Ok();
 }
 
@@ -197,6 +208,8 @@ void Ctx::destroy()
     fork = join = join2 = join3 = nullptr;
     delete stage;
     stage = nullptr;
+    delete stage2;
+    stage2 = nullptr;
 }
 
 Status Engine::init()

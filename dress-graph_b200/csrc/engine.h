@@ -106,6 +106,7 @@ struct Ctx {
     cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr, join3 = nullptr;
     const dressx_config_t *cfg = nullptr;
     Pinned *stage = nullptr;               // host staging of this context's uploads and downloads
+    Pinned *stage2 = nullptr;              // a second stage: an upload on a host thread of its own
     // priority: CUDA stream priority of both streams (0 = default; lower
     // numbers are served first by the block scheduler)
     Status create(int dev, int sms, const dressx_config_t *config, int priority = 0);
@@ -161,6 +162,9 @@ struct HostSpan {
 constexpr size_t STAGE_CHUNK = (size_t)32 << 20;
 Status staged_upload(const HostSpan *spans, int n, const Ctx &ctx);
 Status staged_download(const HostSpan *spans, int n, const Ctx &ctx);
+// the same upload through a given stage, on a given stream (the caller's
+// thread must have the stream's device current)
+Status staged_upload_via(const HostSpan *spans, int n, Pinned *stage, cudaStream_t st);
 
 // ---- device utilities (scan.cu) -------------------------------------------
 // out[i] = sum_{j<i} in[i] for i in [0, n], out[n] = total.  `tmp` must hold

@@ -28,6 +28,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -55,27 +56,43 @@ __device__ __forceinline__ unsigned lanemask_lt()
 
 // flags[0]: malformed input, flags[1]: a row repeats a neighbour,
 // flags[2]: edge weights are not all bit-identical, flags[3]: max row length.
-__global__ void k_validate_rows(int N, int E, const int *off, const int *tgt, const int *eidx,
+// One warp per row (a hub's row is spread over the lanes).  A row outside
+// [0, S) or with end < begin is flagged and not read, so a malformed
+// adj_offset never leads to a read outside adj_target.
+__global__ void k_validate_rows(int N, int E, long long S, const int *off, const int *tgt, const int *eidx,
                                 int *deg, int *flags)
 {
-    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
-        int b = off[u], e = off[u + 1];
-        if (e < b) { atomicOr(&flags[0], 1); deg[u] = 0; continue; }
-        deg[u] = e - b;
-        atomicMax(&flags[3], e - b);
-        int prev = -1;
-        for (int s = b; s < e; ++s) {
-            int x = tgt[s], ei = eidx[s];
-            if (x < 0 || x >= N || ei < 0 || ei >= E) { atomicOr(&flags[0], 2); break; }
-            if (s > b) {
-                if (x == prev) flags[1] = 1;
-                else if (x < prev) atomicOr(&flags[0], 4);
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    int rmax = 0, bad = 0, dup = 0;
+    for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < N; u += nw) {
+        const long long b = off[u], e = off[u + 1];
+        if (e < b || b < 0 || e > S) {
+            bad |= 1;
+            if (lane == 0) deg[u] = 0;
+            continue;
+        }
+        if (lane == 0) deg[u] = (int)(e - b);
+        rmax = max(rmax, (int)(e - b));
+        for (long long q = b + lane; q < e; q += 32) {
+            const int x = tgt[q], ei = eidx[q];
+            if (x < 0 || x >= N || ei < 0 || ei >= E) bad |= 2;
+            if (q > b) {
+                const int prev = tgt[q - 1];
+                if (x == prev) dup = 1;
+                else if (x < prev) bad |= 4;
             }
-            prev = x;
         }
     }
+    rmax = __reduce_max_sync(0xffffffffu, rmax);
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    dup = __reduce_or_sync(0xffffffffu, dup);
+    if (lane == 0) {
+        if (bad) atomicOr(&flags[0], bad);
+        if (dup) flags[1] = 1;
+        if (rmax) atomicMax(&flags[3], rmax);
+    }
 }
-
 __global__ void k_validate_edges(int N, int E, const int *U, const int *V, const double *w, int *flags)
 {
     unsigned long long w0 = E > 0 ? (unsigned long long)__double_as_longlong(w[0]) : 0ULL;
@@ -139,25 +156,45 @@ __device__ __forceinline__ unsigned long long rank_key(const int *deg, int v)
     return ((unsigned long long)(unsigned)deg[v] << 32) | (unsigned)v;
 }
 
+// The oriented rows: the neighbours of higher (degree, id) rank, in row
+// order (ascending id).  One warp per row; the fill compacts by ballot.
 __global__ void k_orient_count(int N, const int *off, const int *tgt, const int *deg, int *ocnt)
 {
-    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
-        unsigned long long ku = rank_key(deg, u);
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < N; u += nw) {
+        const unsigned long long ku = rank_key(deg, u);
         int c = 0;
-        for (int s = off[u]; s < off[u + 1]; ++s) c += rank_key(deg, tgt[s]) > ku;
-        ocnt[u] = c;
+        for (int q = off[u] + lane; q < off[u + 1]; q += 32) c += rank_key(deg, tgt[q]) > ku;
+        c = __reduce_add_sync(0xffffffffu, c);
+        if (lane == 0) ocnt[u] = c;
     }
 }
-
 __global__ void k_orient_fill(int N, const int *off, const int *tgt, const int *eidx, const int *deg,
                               const long long *ooff, int *otgt, int *oeid, int *osrc)
 {
-    for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < N; u += gridDim.x * blockDim.x) {
-        unsigned long long ku = rank_key(deg, u);
-        long long q = ooff[u];
-        for (int s = off[u]; s < off[u + 1]; ++s) {
-            int x = tgt[s];
-            if (rank_key(deg, x) > ku) { otgt[q] = x; oeid[q] = eidx[s]; osrc[q] = u; ++q; }
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < N; u += nw) {
+        const unsigned long long ku = rank_key(deg, u);
+        long long o = ooff[u];
+        const int b = off[u], e = off[u + 1];
+        for (int q0 = b; q0 < e; q0 += 32) {
+            const int q = q0 + lane;
+            int x = 0;
+            bool keep = false;
+            if (q < e) {
+                x = tgt[q];
+                keep = rank_key(deg, x) > ku;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (keep) {
+                const long long at = o + __popc(m & lanemask_lt());
+                otgt[at] = x;
+                oeid[at] = eidx[q];
+                osrc[at] = u;
+            }
+            o += __popc(m);
         }
     }
 }
@@ -261,14 +298,16 @@ __global__ void k_bin_scatter(int n, const int *len, int *cursor, int *perm, int
 // most edges of its row unless it is a hub, so a row's edges sit in two runs
 // and the (u, x) edges of an edge's common-neighbour pairs next to each
 // other: neighbouring lanes gather neighbouring products.
+// vb: bits of a vertex id (the keys take 2 vb + 1 bits, so the radix sort
+// skips the passes over their zero high bytes)
 __global__ void k_edge_keys(int E, const int *U, const int *V, const int *deg, const int *vinv, const int *cnt,
-                            unsigned long long *keys, unsigned *vals)
+                            int vb, unsigned long long *keys, unsigned *vals)
 {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
         const int u = U[e], v = V[e];
         const bool uo = rank_key(deg, u) <= rank_key(deg, v);
         const unsigned long long o = (unsigned)vinv[uo ? u : v], x = (unsigned)vinv[uo ? v : u];
-        keys[e] = ((unsigned long long)(cnt[e] > 0) << 62) | (o << 31) | x;
+        keys[e] = ((unsigned long long)(cnt[e] > 0) << (2 * vb)) | (o << vb) | x;
         vals[e] = (unsigned)e;
     }
 }
@@ -283,7 +322,7 @@ __device__ __forceinline__ unsigned pair_class(int n)
 __global__ void k_class_keys(int e0, int E, const int *ncnt, unsigned long long *keys, unsigned *vals)
 {
     for (int j = e0 + blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
-        keys[j - e0] = ((unsigned long long)pair_class(ncnt[j]) << 32) | (unsigned)j;
+        keys[j - e0] = pair_class(ncnt[j]);    // stable sort: ids stay ascending per class
         vals[j - e0] = (unsigned)j;
     }
 }
@@ -293,7 +332,7 @@ __global__ void k_class_bounds(int n, const unsigned long long *keys, int *bound
 {
     const int c = threadIdx.x;
     if (c > 6) return;
-    const unsigned long long want = (unsigned long long)c << 32;
+    const unsigned long long want = (unsigned long long)c;
     int lo = 0, hi = n;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
@@ -316,24 +355,104 @@ __global__ void k_inverse(int n, const unsigned *perm, int *pinv, int *inv)
     }
 }
 
-// pairs of each edge keyed (edge, e_ux): a sort groups them by edge (in
-// order, so the offsets stay) and orders each edge's pairs by e_ux
-__global__ void k_pair_keys(int E, const long long *ioff, const int2 *pairs, unsigned long long *keys, unsigned *vals)
+// Each edge's pairs put in (first, second) edge-id order, in place: a
+// warp's lanes then gather neighbouring products (an owner's edges are
+// contiguous).  The order only serves locality -- the certified sums give the
+// same bits in any order -- so edges past BIG_CAP pairs keep theirs.
+__device__ __forceinline__ unsigned long long pair_word(int2 pr)
 {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
-        const long long b = ioff[j], n = ioff[j + 1] - b;
-        for (long long k = 0; k < n; ++k) {
-            const int2 pr = pairs[b + k];
-            keys[b + k] = ((unsigned long long)(unsigned)j << 32) | (unsigned)pr.x;
-            vals[b + k] = (unsigned)pr.y;
+    return ((unsigned long long)(unsigned)pr.x << 32) | (unsigned)pr.y;
+}
+__device__ __forceinline__ int2 word_pair(unsigned long long w)
+{
+    return make_int2((int)(unsigned)(w >> 32), (int)(unsigned)w);
+}
+
+// up to 16 pairs: one thread per edge, insertion sort
+__global__ void k_sort_pairs_thr(const int *list, int begin, int end, const long long *ioff, int2 *pairs)
+{
+    for (int x = begin + blockIdx.x * blockDim.x + threadIdx.x; x < end; x += gridDim.x * blockDim.x) {
+        const int j = list[x];
+        const long long b = ioff[j];
+        const int n = (int)(ioff[j + 1] - b);
+        unsigned long long w[16];
+        for (int k = 0; k < n && k < 16; ++k) {
+            const unsigned long long t = pair_word(pairs[b + k]);
+            int i = k;
+            for (; i > 0 && w[i - 1] > t; --i) w[i] = w[i - 1];
+            w[i] = t;
         }
+        for (int k = 0; k < n && k < 16; ++k) pairs[b + k] = word_pair(w[k]);
     }
 }
 
-__global__ void k_pairs_from_keys(long long T, const unsigned long long *keys, const unsigned *vals, int2 *pairs)
+// bitonic sort of buf[0, P) (P a power of two) by `nt` cooperating threads
+template <bool BLOCK>
+__device__ __forceinline__ void bitonic(unsigned long long *buf, int P, int tid, int nt)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < T; i += (long long)gridDim.x * blockDim.x)
-        pairs[i] = make_int2((int)(unsigned)(keys[i] & 0xffffffffULL), (int)vals[i]);
+    for (int k = 2; k <= P; k <<= 1)
+        for (int h = k >> 1; h > 0; h >>= 1) {
+            for (int i = tid; i < P; i += nt) {
+                const int o = i ^ h;
+                if (o > i) {
+                    const unsigned long long a = buf[i], c = buf[o];
+                    if ((a > c) == ((i & k) == 0)) {
+                        buf[i] = c;
+                        buf[o] = a;
+                    }
+                }
+            }
+            if (BLOCK) __syncthreads();
+            else __syncwarp();
+        }
+}
+
+constexpr int SORT_WARP_CAP = MED_CAP;     // pairs a warp sorts in shared memory
+constexpr int SORT_WARPS = 8;
+
+// 17..MED_CAP pairs: one warp per edge
+__global__ void __launch_bounds__(32 * SORT_WARPS) k_sort_pairs_warp(const int *list, int begin, int end,
+                                                                    const long long *ioff, int2 *pairs)
+{
+    __shared__ unsigned long long sb[SORT_WARPS][SORT_WARP_CAP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long *buf = sb[wid];
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int x = begin + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); x < end; x += nw) {
+        const int j = list[x];
+        const long long b = ioff[j];
+        const int n = (int)(ioff[j + 1] - b);
+        if (n > SORT_WARP_CAP) continue;
+        int P = 32;
+        while (P < n) P <<= 1;
+        for (int k = lane; k < P; k += 32) buf[k] = k < n ? pair_word(pairs[b + k]) : ~0ULL;
+        __syncwarp();
+        bitonic<false>(buf, P, lane, 32);
+        for (int k = lane; k < n; k += 32) pairs[b + k] = word_pair(buf[k]);
+        __syncwarp();
+    }
+}
+
+constexpr int SORT_BLK_THR = 512;
+
+// MED_CAP+1..BIG_CAP pairs: one block per edge
+__global__ void __launch_bounds__(SORT_BLK_THR) k_sort_pairs_blk(const int *list, int begin, int end,
+                                                                 const long long *ioff, int2 *pairs)
+{
+    __shared__ unsigned long long buf[BIG_CAP];
+    for (int x = begin + (int)blockIdx.x; x < end; x += gridDim.x) {
+        const int j = list[x];
+        const long long b = ioff[j];
+        const int n = (int)(ioff[j + 1] - b);
+        if (n > BIG_CAP) continue;
+        int P = 32;
+        while (P < n) P <<= 1;
+        for (int k = threadIdx.x; k < P; k += blockDim.x) buf[k] = k < n ? pair_word(pairs[b + k]) : ~0ULL;
+        __syncthreads();
+        bitonic<true>(buf, P, threadIdx.x, blockDim.x);
+        for (int k = threadIdx.x; k < n; k += blockDim.x) pairs[b + k] = word_pair(buf[k]);
+        __syncthreads();
+    }
 }
 
 __global__ void k_gather_seg(int n, const int *perm, const int *len, int *out)
@@ -367,109 +486,6 @@ __global__ void k_new_rows(int N, const int *vperm, const int *off, const int *e
     }
 }
 
-// ---- the second copy of the products (large simple undirected graphs) ----
-// Every edge with common neighbours has an owner (the endpoint of lower
-// (degree, id) rank) and a non-owner.  Its product lives at its id, in the
-// owner's runs; the vertex phase also writes it, as it gathers it anyway,
-// into a copy area Q after the E products, at qpos[e], inside the
-// non-owner's contiguous run [qbeg[v], qbeg[v+1]).  The common-neighbour
-// pair (e_ux, e_vx) of edge (u, v) then refers to e_ux in u's data -- its
-// id if u owns it, E + qpos[e_ux] if not -- and to e_vx in v's data, so the
-// gathers of an edge fall into four contiguous runs instead of scattering
-// over the array.
-
-// owner of every edge, in the new numbering of edges and vertices
-__global__ void k_edge_owner(int E, const int *eperm, const int *U, const int *V, const int *deg, const int *vinv,
-                             int *own)
-{
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
-        const int e = eperm[j], u = U[e], v = V[e];
-        own[j] = vinv[rank_key(deg, u) <= rank_key(deg, v) ? u : v];
-    }
-}
-
-// slot class of new vertex i's slot with new edge id en: 0 owned by i,
-// 1 not owned and with common neighbours (ids from e0 on), 2 the rest
-__device__ __forceinline__ int slot_class(int en, int i, const int *own, int e0)
-{
-    return own[en] == i ? 0 : en >= e0 ? 1 : 2;
-}
-
-// per new vertex: its slots of class 1 (one warp per vertex)
-__global__ void k_q_count(int N, const int *vperm, const int *off, const int *eidx, const int *einv, const int *own,
-                          int e0, int *nq)
-{
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
-        const int u = vperm[i], b = off[u], n = off[u + 1] - b;
-        int c = 0;
-        for (int k = lane; k < n; k += 32) c += slot_class(einv[eidx[b + k]], i, own, e0) == 1;
-        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-        if (lane == 0) nq[i] = c;
-    }
-}
-
-// the new rows, each stably partitioned into its class 0, 1, 2 slots; the
-// class-1 slots get their copy positions, rq[i] is where they start in the row
-__global__ void k_new_rows_q(int N, const int *vperm, const int *off, const int *eidx, const int *einv,
-                             const int *own, int e0, const long long *row_off, const long long *qbeg, int *row_eid,
-                             int *qpos, int *rq, const double *nw_in, double *nw_out)
-{
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    unsigned lt;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < N; i += warps) {
-        const int u = vperm[i], b = off[u], n = off[u + 1] - b;
-        int n0 = 0;
-        for (int k = lane; k < n; k += 32) n0 += slot_class(einv[eidx[b + k]], i, own, e0) == 0;
-        for (int o = 16; o > 0; o >>= 1) n0 += __shfl_xor_sync(0xffffffffu, n0, o);
-        const int n1 = (int)(qbeg[i + 1] - qbeg[i]);
-        int at[3] = {0, n0, n0 + n1};
-        const long long o = row_off[i];
-        for (int k0 = 0; k0 < n; k0 += 32) {
-            const int k = k0 + lane;
-            const int en = k < n ? einv[eidx[b + k]] : -1;
-            const int c = k < n ? slot_class(en, i, own, e0) : 3;
-            const unsigned m0 = __ballot_sync(0xffffffffu, c == 0), m1 = __ballot_sync(0xffffffffu, c == 1),
-                           m2 = __ballot_sync(0xffffffffu, c == 2);
-            if (c < 3) {
-                const unsigned m = c == 0 ? m0 : c == 1 ? m1 : m2;
-                const int pos = at[c] + __popc(m & lt);
-                row_eid[o + pos] = en;
-                if (c == 1) qpos[en] = (int)qbeg[i] + (pos - n0);
-            }
-            at[0] += __popc(m0);
-            at[1] += __popc(m1);
-            at[2] += __popc(m2);
-        }
-        if (lane == 0) {
-            rq[i] = n0;
-            nw_out[i] = nw_in[u];
-        }
-    }
-}
-
-// the pairs of every edge as references into the products and their copy:
-// the side sharing u (v) read from u's (v's) data
-__global__ void k_pair_refs(int E, const long long *ioff, const int *eu, const int *ev, const int *own,
-                            const int *qpos, int2 *pairs)
-{
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
-        const int u = eu[j], v = ev[j];
-        const long long b = ioff[j], n = ioff[j + 1] - b;
-        for (long long k = 0; k < n; ++k) {
-            const int2 pr = pairs[b + k];
-            const bool xu = eu[pr.x] == u || ev[pr.x] == u;
-            const int au = xu ? pr.x : pr.y, av = xu ? pr.y : pr.x;
-            const int ru = own[au] == u ? au : E + qpos[au];
-            const int rv = own[av] == v ? av : E + qpos[av];
-            pairs[b + k] = make_int2(ru, rv);
-        }
-    }
-}
-
 __global__ void k_new_edges(int E, const int *eperm, const int *U, const int *V, const int *vinv,
                             const double *w, const double *d, const int *cnt, int *eu, int *ev,
                             double *wn, double *d0, double *p0, int *ncnt)
@@ -485,14 +501,20 @@ __global__ void k_new_edges(int E, const int *eperm, const int *U, const int *V,
     }
 }
 
-__global__ void k_new_pairs(int E, const int *eperm, const long long *ioff_old, const int2 *pairs_old,
-                            const int *einv, const long long *ioff_new, int2 *pairs_new)
+// The pairs of the edges in list[lo, hi), copied to their new places with
+// the new edge ids: GW lanes per edge (1 for the short classes, a warp for
+// edges of 17 pairs or more, so a long edge is not one thread's loop).
+template <int GW>
+__global__ void k_new_pairs(const int *list, int lo, int hi, const int *eperm, const long long *ioff_old,
+                            const int2 *pairs_old, const int *einv, const long long *ioff_new, int2 *pairs_new)
 {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < E; j += gridDim.x * blockDim.x) {
-        int e = eperm[j];
-        long long a = ioff_old[e], n = ioff_old[e + 1] - a, o = ioff_new[j];
-        for (long long k = 0; k < n; ++k) {
-            int2 pr = pairs_old[a + k];
+    const int lane = threadIdx.x & (GW - 1);
+    const long long ng = ((long long)gridDim.x * blockDim.x) / GW;
+    for (long long x = lo + (blockIdx.x * (long long)blockDim.x + threadIdx.x) / GW; x < hi; x += ng) {
+        const int j = list[x], e = eperm[j];
+        const long long a = ioff_old[e], n = ioff_old[e + 1] - a, o = ioff_new[j];
+        for (long long k = lane; k < n; k += GW) {
+            const int2 pr = pairs_old[a + k];
             pairs_new[o + k] = make_int2(einv[pr.x], einv[pr.y]);
         }
     }
@@ -508,6 +530,51 @@ __global__ void k_unpermute(int n, const int *perm, const double *src, double *d
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         dst[perm[i]] = src[i];
 }
+
+// An upload on a host thread of its own, through the context's second stage
+// on stream side2: started before the kernels that need only the CSR, joined
+// before the first that reads its arrays.  The destructor joins, so no early
+// return leaves the thread running.
+struct BackgroundUpload {
+    std::thread th;
+    Status result;
+    bool running = false;
+    double wait_ms = 0.0;                  // time the caller spent blocked in join()
+    Status start(std::vector<HostSpan> spans, const Ctx &ctx)
+    {
+        // the destination buffers were allocated in stream order on ctx.st
+        DRESS_CUDA_TRY(cudaEventRecord(ctx.fork, ctx.st));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(ctx.side2, ctx.fork, 0));
+        try {
+            th = std::thread([this, sp = std::move(spans), &ctx]() {
+                const cudaError_t e = cudaSetDevice(ctx.device);
+                if (e != cudaSuccess) {
+                    result = Status::Err(DRESSX_ECUDA, cudaGetErrorString(e));
+                    return;
+                }
+                result = staged_upload_via(sp.data(), (int)sp.size(), ctx.stage2, ctx.side2);
+            });
+        } catch (...) {
+            return Status::Err(DRESSX_ENOMEM, "cannot start the upload thread");
+        }
+        running = true;
+        return Status::Ok();
+    }
+    Status join()
+    {
+        if (running) {
+            const auto w0 = std::chrono::steady_clock::now();
+            th.join();
+            running = false;
+            wait_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
+        }
+        return result;
+    }
+    ~BackgroundUpload()
+    {
+        if (running) th.join();
+    }
+};
 
 double ms_since(std::chrono::steady_clock::time_point t0)
 {
@@ -545,7 +612,8 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     const int sms = ctx.num_sms;
     const int fwd = (g->variant == DRESS_VARIANT_FORWARD || g->variant == DRESS_VARIANT_BACKWARD);
 
-    // ---- upload: every array through the pinned stage in one pipeline ------
+    // ---- upload: the CSR first; the edge arrays on a host thread of their
+    // own, beside the row validation and the triangle listing (CSR only) --------
     DevBuf<int> d_off, d_tgt, d_eidx, d_U, d_V;
     DevBuf<double> d_w, d_d, d_nw;
     DRESS_TRY(d_off.alloc((size_t)N + 1, st));
@@ -557,41 +625,60 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_d.alloc((size_t)E, st));
     DRESS_TRY(d_nw.alloc((size_t)N, st));
     {
-        std::vector<HostSpan> spans = {
-            {g->adj_offset, d_off.get(), ((size_t)N + 1) * sizeof(int)},
-            {g->adj_target, d_tgt.get(), (size_t)S * sizeof(int)},
-            {g->adj_edge_idx, d_eidx.get(), (size_t)S * sizeof(int)},
-            {g->U, d_U.get(), (size_t)E * sizeof(int)},
-            {g->V, d_V.get(), (size_t)E * sizeof(int)},
-            {g->edge_weight, d_w.get(), (size_t)E * sizeof(double)},
-            {g->edge_dress, d_d.get(), (size_t)E * sizeof(double)}};
+        const HostSpan csr[3] = {{g->adj_offset, d_off.get(), ((size_t)N + 1) * sizeof(int)},
+                                 {g->adj_target, d_tgt.get(), (size_t)S * sizeof(int)},
+                                 {g->adj_edge_idx, d_eidx.get(), (size_t)S * sizeof(int)}};
+        DRESS_TRY(staged_upload(csr, 3, ctx));
+    }
+    BackgroundUpload edge_up;
+    {
+        std::vector<HostSpan> spans = {{g->U, d_U.get(), (size_t)E * sizeof(int)},
+                                       {g->V, d_V.get(), (size_t)E * sizeof(int)},
+                                       {g->edge_weight, d_w.get(), (size_t)E * sizeof(double)},
+                                       {g->edge_dress, d_d.get(), (size_t)E * sizeof(double)}};
         if (g->NW) spans.push_back({g->NW, d_nw.get(), (size_t)N * sizeof(double)});
-        DRESS_TRY(staged_upload(spans.data(), (int)spans.size(), ctx));
+        DRESS_TRY(edge_up.start(std::move(spans), ctx));
     }
     const double t_upload = ms_since(t0);
     if (!g->NW && N)                           // NULL vertex weights mean all 1.0
         count_launch(), k_fill<<<grid_for(N, 256, 16 * sms), 256, 0, st>>>(N, 1.0, d_nw.get());
 
-    // ---- validate ----------------------------------------------------------
+    // ---- validate the rows ---------------------------------------------------
     DevBuf<int> d_flags, d_deg, d_cnt;
     DRESS_TRY(d_flags.alloc(8, st));
     DRESS_TRY(d_deg.alloc((size_t)N, st));
     DRESS_TRY(d_cnt.alloc((size_t)E, st));
     DRESS_CUDA_TRY(cudaMemsetAsync(d_flags.get(), 0, 8 * sizeof(int), st));
-    count_launch(), k_validate_rows<<<grid_for(N, 256, 16 * sms), 256, 0, st>>>(N, E, d_off.get(), d_tgt.get(),
-                                                                d_eidx.get(), d_deg.get(), d_flags.get());
-    count_launch(), k_validate_edges<<<grid_for(E, 256, 16 * sms), 256, 0, st>>>(N, E, d_U.get(), d_V.get(), d_w.get(),
-                                                                 d_flags.get());
+    count_launch(), k_validate_rows<<<grid_for((long long)N * 32, 256, 16 * sms), 256, 0, st>>>(
+        N, E, S, d_off.get(), d_tgt.get(), d_eidx.get(), d_deg.get(), d_flags.get());
     DRESS_CUDA_TRY(cudaGetLastError());
     int flags[8];
     DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
     DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-    const double t_validate = ms_since(t0);
+    double t_valid = ms_since(t0) - t_upload;
     if (flags[0]) return Status::Err(DRESSX_EINVAL, "malformed graph (CSR or edge endpoints out of range)");
     const bool dup = flags[1] != 0;
-    const bool uniform = flags[2] == 0;
-    const double wc = E > 0 ? g->edge_weight[0] : 1.0;
     const long long max_row = flags[3];
+    const double wc = E > 0 ? g->edge_weight[0] : 1.0;
+    // The edge arrays, validated once they are on the device: before the
+    // pairs unless the triangle listing (CSR only) makes them.
+    bool uniform = true;
+    auto validate_edges = [&]() -> Status {
+        DRESS_TRY(edge_up.join());
+        const auto v0 = std::chrono::steady_clock::now();
+        count_launch(), k_validate_edges<<<grid_for(E, 256, 16 * sms), 256, 0, st>>>(N, E, d_U.get(), d_V.get(),
+                                                                                      d_w.get(), d_flags.get());
+        DRESS_CUDA_TRY(cudaGetLastError());
+        DRESS_CUDA_TRY(counted_memcpy(flags, d_flags.get(), sizeof(flags), cudaMemcpyDeviceToHost, st));
+        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+        t_valid += ms_since(v0);
+        if (flags[0]) return Status::Err(DRESSX_EINVAL, "malformed graph (CSR or edge endpoints out of range)");
+        uniform = flags[2] == 0;
+        return Status::Ok();
+    };
+    const bool tri_path = !(g->precompute_intercepts && g->intercept_offset) &&
+                          g->variant == DRESS_VARIANT_UNDIRECTED && !dup;
+    if (!tri_path) DRESS_TRY(validate_edges());
 
     // ---- common-neighbour tables (original edge ids) -------------------------
     DevBuf<long long> d_ioff_old, d_scan_tmp;
@@ -627,7 +714,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         DRESS_TRY(d_otgt.alloc((size_t)(S > 0 ? S : 1), st));
         DRESS_TRY(d_oeid.alloc((size_t)(S > 0 ? S : 1), st));
         DRESS_TRY(d_osrc.alloc((size_t)(S > 0 ? S : 1), st));
-        const int vg = (int)grid_for(N, 256, 32 * sms);
+        const int vg = (int)grid_for((long long)N * 32, 256, 32 * sms);     // a warp per row
         count_launch(), k_orient_count<<<vg, 256, 0, st>>>(N, d_off.get(), d_tgt.get(), d_deg.get(), d_ocnt.get());
         DRESS_TRY(exclusive_scan_i32(d_ocnt.get(), d_ooff.get(), N, d_scan_tmp.get(), st));
         count_launch(), k_orient_fill<<<vg, 256, 0, st>>>(N, d_off.get(), d_tgt.get(), d_eidx.get(), d_deg.get(),
@@ -659,6 +746,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
                                                       d_pairs_old.get());
     }
     DRESS_CUDA_TRY(cudaGetLastError());
+    if (tri_path) DRESS_TRY(validate_edges());
     d_tgt.release();
 
     // ---- bins and renumbering ---------------------------------------------------
@@ -725,8 +813,10 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         DRESS_TRY(k1.alloc((size_t)E, st));
         DRESS_TRY(v0.alloc((size_t)E, st));
         DRESS_TRY(v1.alloc((size_t)E, st));
+        int vbits = 1;
+        while (vbits < 31 && (1LL << vbits) < (long long)N) ++vbits;
         count_launch(), k_edge_keys<<<eg, 256, 0, st>>>(E, d_U.get(), d_V.get(), d_deg.get(), d_vinv.get(),
-                                                        d_cnt.get(), k0.get(), v0.get());
+                                                        d_cnt.get(), vbits, k0.get(), v0.get());
         unsigned long long *sk = nullptr;
         unsigned *sv = nullptr;
         DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), E, &sk, &sv, st, sms));
@@ -770,52 +860,19 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_TRY(d_nwi.alloc((size_t)N, st));
     count_launch(), k_gather_deg<<<vg, 256, 0, st>>>(N, d_vperm.get(), d_deg.get(), d_ndeg.get());
     DRESS_TRY(exclusive_scan_i32(d_ndeg.get(), d_row_off.get(), N, d_scan_tmp.get(), st));
-    // The second copy of the products (see k_pair_refs): large simple
-    // undirected graphs, whose pairs come from the triangle listing.
-    const bool qmode = locality && !(g->precompute_intercepts && g->intercept_offset) &&
-                       g->variant == DRESS_VARIANT_UNDIRECTED && !dup && E - eb.count(B0) > 0;
-    DevBuf<int> d_own, d_qpos, d_rq, d_nq;
-    DevBuf<long long> d_qbeg;
-    long long Qn = 0;
-    if (qmode) {
-        const int e0q = eb.count(B0);
-        DRESS_TRY(d_own.alloc((size_t)E, st));
-        DRESS_TRY(d_qpos.alloc((size_t)E, st));
-        DRESS_TRY(d_rq.alloc((size_t)N, st));
-        DRESS_TRY(d_nq.alloc((size_t)N, st));
-        DRESS_TRY(d_qbeg.alloc((size_t)N + 1, st));
-        count_launch(), k_edge_owner<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_U.get(), d_V.get(), d_deg.get(),
-                                                         d_vinv.get(), d_own.get());
-        const unsigned wg = grid_for((long long)N * 32, 256, 64 * sms);
-        count_launch(), k_q_count<<<wg, 256, 0, st>>>(N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(),
-                                                      d_own.get(), e0q, d_nq.get());
-        DRESS_TRY(exclusive_scan_i32(d_nq.get(), d_qbeg.get(), N, d_scan_tmp.get(), st));
-        count_launch(), k_new_rows_q<<<wg, 256, 0, st>>>(N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(),
-                                                         d_own.get(), e0q, d_row_off.get(), d_qbeg.get(),
-                                                         d_row_eid.get(), d_qpos.get(), d_rq.get(), d_nw.get(),
-                                                         d_nwi.get());
-        DRESS_CUDA_TRY(counted_memcpy(&Qn, d_qbeg.get() + N, sizeof(Qn), cudaMemcpyDeviceToHost, st));
-        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-        d_nq.release();
-    } else {
-        count_launch(), k_new_rows<<<grid_for((long long)N * 32, 256, 64 * sms), 256, 0, st>>>(
-            N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(), d_row_off.get(), d_row_eid.get(),
-            d_nw.get(), d_nwi.get());
-    }
+    count_launch(), k_new_rows<<<grid_for((long long)N * 32, 256, 64 * sms), 256, 0, st>>>(
+        N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(), d_row_off.get(), d_row_eid.get(),
+        d_nw.get(), d_nwi.get());
     d_eidx.release();
     d_ndeg.release();
-    // value and product buffers: E entries, then the copy area (uniform
-    // weights gather the values, other graphs the products)
-    const size_t dstride = (size_t)E + (uniform ? (size_t)Qn : 0);
-    const size_t pstride = (size_t)E + (size_t)Qn;
 
     DRESS_TRY(d_eu.alloc((size_t)E, st));
     DRESS_TRY(d_ev.alloc((size_t)E, st));
     DRESS_TRY(d_ncnt.alloc((size_t)E, st));
-    DRESS_TRY(d_dbuf.alloc(2 * dstride, st));
+    DRESS_TRY(d_dbuf.alloc(2 * (size_t)E, st));
     if (!uniform) {
         DRESS_TRY(d_wi.alloc((size_t)E, st));
-        DRESS_TRY(d_pbuf.alloc(2 * pstride, st));
+        DRESS_TRY(d_pbuf.alloc(2 * (size_t)E, st));
     }
     count_launch(), k_new_edges<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_U.get(), d_V.get(), d_vinv.get(), d_w.get(),
                                     d_d.get(), d_cnt.get(), d_eu.get(), d_ev.get(),
@@ -866,30 +923,32 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     }
     ec.list = d_elist.get();
     DRESS_TRY(d_pairs.alloc((size_t)(T > 0 ? T : 1), st));
-    count_launch(), k_new_pairs<<<eg, 256, 0, st>>>(E, d_eperm.get(), d_ioff_old.get(), d_pairs_old.get(), d_einv.get(),
-                                    d_ioff.get(), d_pairs.get());
-    if (qmode) {
-        count_launch(), k_pair_refs<<<eg, 256, 0, st>>>(E, d_ioff.get(), d_eu.get(), d_ev.get(), d_own.get(),
-                                                        d_qpos.get(), d_pairs.get());
-        d_own.release();
-        d_qpos.release();
+    if (E - e0 > 0) {
+        const int c1 = ec.cls[1], c6 = ec.cls[6];
+        if (c1 > 0)
+            count_launch(), k_new_pairs<1><<<grid_for(c1, 256, 64 * sms), 256, 0, st>>>(
+                ec.list, 0, c1, d_eperm.get(), d_ioff_old.get(), d_pairs_old.get(), d_einv.get(), d_ioff.get(),
+                d_pairs.get());
+        if (c6 > c1)
+            count_launch(), k_new_pairs<32><<<grid_for((long long)(c6 - c1) * 32, 256, 64 * sms), 256, 0, st>>>(
+                ec.list, c1, c6, d_eperm.get(), d_ioff_old.get(), d_pairs_old.get(), d_einv.get(), d_ioff.get(),
+                d_pairs.get());
     }
     DRESS_CUDA_TRY(cudaGetLastError());
     d_pairs_old.release();
-    // each edge's pairs in e_ux order: a warp's lanes then gather neighbouring
-    // products (an owner's edges are contiguous)
+    // each edge's pairs in edge-id order (class lists: thread, warp and block sorts)
     if (locality && T > 1) {
-        DevBuf<unsigned long long> k0, k1;
-        DevBuf<unsigned> v0, v1;
-        DRESS_TRY(k0.alloc((size_t)T, st));
-        DRESS_TRY(k1.alloc((size_t)T, st));
-        DRESS_TRY(v0.alloc((size_t)T, st));
-        DRESS_TRY(v1.alloc((size_t)T, st));
-        count_launch(), k_pair_keys<<<eg, 256, 0, st>>>(E, d_ioff.get(), d_pairs.get(), k0.get(), v0.get());
-        unsigned long long *sk = nullptr;
-        unsigned *sv = nullptr;
-        DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), T, &sk, &sv, st, sms));
-        count_launch(), k_pairs_from_keys<<<grid_for(T, 256, 64 * sms), 256, 0, st>>>(T, sk, sv, d_pairs.get());
+        const int *L = ec.list;
+        const int c0 = ec.cls[0], c1 = ec.cls[1], c4 = ec.cls[4], c5 = ec.cls[5];
+        if (c1 > c0)
+            count_launch(), k_sort_pairs_thr<<<grid_for(c1 - c0, 256, 64 * sms), 256, 0, st>>>(L, c0, c1, d_ioff.get(),
+                                                                                             d_pairs.get());
+        if (c4 > c1)
+            count_launch(), k_sort_pairs_warp<<<grid_for((long long)(c4 - c1) * 32, 32 * SORT_WARPS, 32 * sms),
+                                               32 * SORT_WARPS, 0, st>>>(L, c1, c4, d_ioff.get(), d_pairs.get());
+        if (c5 > c4)
+            count_launch(), k_sort_pairs_blk<<<(unsigned)std::min(c5 - c4, 8 * sms), SORT_BLK_THR, 0, st>>>(
+                L, c4, c5, d_ioff.get(), d_pairs.get());
         DRESS_CUDA_TRY(cudaGetLastError());
     }
     d_U.release(); d_V.release(); d_w.release(); d_d.release(); d_nw.release();
@@ -946,11 +1005,8 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     DRESS_CUDA_TRY(cudaMemsetAsync(d_qcount.get(), 0, 2 * sizeof(unsigned), st));
     s.qv = d_qv.get(); s.qe = d_qe.get(); s.qcount = d_qcount.get();
     LaunchCfg lc{sms, exact_grid, exact_smem, st, ctx.side, ctx.fork, ctx.join};
-    double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + dstride};
-    double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + pstride};
-    s.qbeg = qmode ? d_qbeg.get() : nullptr;
-    s.qw = nullptr;
-    s.rq = qmode ? d_rq.get() : nullptr;
+    double *dbuf[2] = {d_dbuf.get(), d_dbuf.get() + E};
+    double *pbuf[2] = {uniform ? nullptr : d_pbuf.get(), uniform ? nullptr : d_pbuf.get() + E};
 
     // Two sweeps (the even one writes buffer 1, the odd one buffer 0) and the
     // index steps between them are captured once into a CUDA graph, replayed
@@ -965,7 +1021,6 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     for (int par = 0; par < 2; ++par) {
         sw2[par].d = dbuf[par]; sw2[par].dn = dbuf[par ^ 1];
         sw2[par].p = pbuf[par]; sw2[par].pn = pbuf[par ^ 1];
-        sw2[par].qw = qmode ? (uniform ? dbuf[par] : pbuf[par]) + E : nullptr;
     }
     auto enqueue_pair = [&]() -> Status {
         for (int par = 0; par < 2; ++par) {
@@ -1074,9 +1129,9 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         stats->sweeps = last + 1;
         stats->setup_ms = setup_ms;
         stats->iterate_ms = sweep_ms;
-        stats->phase_ms[0] = t_upload;
-        stats->phase_ms[1] = t_validate - t_upload;
-        stats->phase_ms[2] = t_pairs - t_validate;
+        stats->phase_ms[0] = t_upload + edge_up.wait_ms;
+        stats->phase_ms[1] = t_valid;
+        stats->phase_ms[2] = t_pairs - t_upload - edge_up.wait_ms - t_valid;
         stats->phase_ms[3] = setup_ms - t_pairs;
         stats->phase_ms[4] = ms_since(t_down0);
     }
