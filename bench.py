@@ -63,6 +63,11 @@ HBM_FALLBACK_GBS = 6650.0
 KBATCH_HEADLINE_NCU = {"dram_bytes": 19.33e6 + 190.33e6,
                        "issue": {"issue_active_frac": 0.724, "lanes_per_inst": 19.5, "fp64_pipe_frac": 0.227}}
 
+# The 28M-edge single fit: dram__bytes_read.sum + dram__bytes_write.sum of the
+# twelve sweep kernels of one sweep (sweep 10), one capture per variant
+# (profiles/single_fit_chunglu28m_sweep_dram.md)
+SINGLE_FIT_NCU = {"edges": 28_000_000, "weighted": 4.286e9 + 0.512e9, "unweighted": 3.925e9 + 0.286e9}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -427,6 +432,7 @@ def bench_single_fit(args, torch):
         # algorithmic bytes per sweep: 24N + 12S + 48E weighted, 24N + 12S + 32E unweighted
         b_iter = 24 * n + 12 * S + (48 if W is not None else 32) * E
         achieved = b_iter / (sweep_ms / 1e3) / 1e9
+        traffic = SINGLE_FIT_NCU[label] if E == SINGLE_FIT_NCU["edges"] else None
         out[label] = {
             "iterations": it, "sweeps": sweeps, "delta": dl, "common_terms": st["common_terms"],
             "edge_iters_per_s": E * sweeps / (st["iterate_ms"] / 1e3),
@@ -434,8 +440,10 @@ def bench_single_fit(args, torch):
             "sweep_ms": sweep_ms, "setup_ms": st["setup_ms"], "e2e_ms": wall * 1e3, "phases_ms": st["phases_ms"],
             "h2d_bytes": cnt["h2d_bytes"], "d2h_bytes": cnt["d2h_bytes"], "launches": cnt["launches"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_sweep": b_iter},
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_sweep": b_iter,
+                         # measured DRAM bytes per sweep over the sweep time: how busy HBM is
+                         "dram_frac": (traffic / (sweep_ms / 1e3) / 1e9 / peak) if traffic else None},
         }
         if gold is not None and label in gold:
             f = gold[label]["full"]
@@ -818,6 +826,7 @@ def compact_sections(single, serving, k2, plain):
                              "setup_ms": _r(v["setup_ms"]), "e2e_ms": _r(v["e2e_ms"])}
                 if v["roofline"].get("traffic"):
                     sf[label]["traffic_gb"] = _r(v["roofline"]["traffic"] / 1e9)
+                    sf[label]["dram_frac"] = _r(v["roofline"]["dram_frac"])
         cb = single.get("cpu_baseline", {}).get("omp")
         if cb:
             sf["cpu_omp_ms_per_sweep"] = _r(cb["ms_per_sweep"])
