@@ -23,7 +23,6 @@
 #include <vector>
 
 #include "engine.h"
-#include <emmintrin.h>
 #include "hist.h"
 #include "host_par.h"
 
@@ -452,30 +451,6 @@ __global__ void k_seg_ends(long long R, const int *run_seg, long long *seg_end)
         if (r + 1 == R || run_seg[r + 1] != run_seg[r]) seg_end[run_seg[r]] = r + 1;
 }
 
-// Copies n 16-byte (value, count) pairs with non-temporal stores: the
-// destination lines are written without being read first, which takes a
-// third of the host memory traffic off the copy out of the pinned stage.
-static void stream_copy16(void *dst, const void *src, size_t n)
-{
-    if (((uintptr_t)dst | (uintptr_t)src) & 15) {
-        std::memcpy(dst, src, n * 16);
-        return;
-    }
-    __m128i *d = (__m128i *)dst;
-    const __m128i *s = (const __m128i *)src;
-    size_t i = 0;
-    for (; i + 4 <= n; i += 4) {
-        const __m128i x0 = _mm_load_si128(s + i), x1 = _mm_load_si128(s + i + 1);
-        const __m128i x2 = _mm_load_si128(s + i + 2), x3 = _mm_load_si128(s + i + 3);
-        _mm_stream_si128(d + i, x0);
-        _mm_stream_si128(d + i + 1, x1);
-        _mm_stream_si128(d + i + 2, x2);
-        _mm_stream_si128(d + i + 3, x3);
-    }
-    for (; i < n; ++i) _mm_stream_si128(d + i, _mm_load_si128(s + i));
-    _mm_sfence();
-}
-
 Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vector<long long> &lens, Pinned *stage,
                        cudaStream_t st, int sms, std::vector<int64_t *> *pre, const std::vector<long long> *cap,
                        int max_threads)
@@ -604,7 +579,7 @@ Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vecto
                 share(sg, a, b);
                 int64_t *o = outs[(size_t)sg];
                 if (b <= a || !o) continue;
-                stream_copy16(o + 2 * (a - first[(size_t)sg]), host + 2 * a, (size_t)(b - a));
+                copy_nt(o + 2 * (a - first[(size_t)sg]), host + 2 * a, (size_t)(b - a) * 16);
             }
         barrier(1);
         // trim the given arrays of the segments starting here (shrinking keeps the data)
