@@ -204,24 +204,31 @@ __global__ void k_orient_fill(int N, const int *off, const int *tgt, const int *
 // the pair of the other two (the order inside a pair is irrelevant: the term
 // is their sum).
 template <bool FILL>
+// The pairs an oriented edge finds for itself go to the head of its own list
+// (own[eab] of them, counted in the first pass), without atomics; the pairs
+// it finds for its triangles' other two edges go through their cursors,
+// which start after those heads.
 __global__ void k_triangles(long long M, const long long *ooff, const int *otgt, const int *oeid,
-                            const int *osrc, int *cnt, unsigned long long *cursor, int2 *pairs)
+                            const int *osrc, int *cnt, int *own_cnt, const long long *ioff,
+                            unsigned long long *cursor, int2 *pairs)
 {
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < M;
          q += (long long)gridDim.x * blockDim.x) {
         int a = osrc[q], b = otgt[q], eab = oeid[q];
         long long pa = ooff[a], pa_end = ooff[a + 1];
         long long pb = ooff[b], pb_end = ooff[b + 1];
+        int own = 0;                           // this edge's triangles so far
+        const long long head = FILL ? ioff[eab] : 0;
         while (pa < pa_end && pb < pb_end) {
             int x = otgt[pa], y = otgt[pb];
             if (x == y) {
                 int eac = oeid[pa], ebc = oeid[pb];
                 if (!FILL) {
-                    atomicAdd(&cnt[eab], 1);
+                    ++own;
                     atomicAdd(&cnt[eac], 1);
                     atomicAdd(&cnt[ebc], 1);
                 } else {
-                    pairs[atomicAdd(&cursor[eab], 1ULL)] = make_int2(eac, ebc);
+                    pairs[head + own++] = make_int2(eac, ebc);
                     pairs[atomicAdd(&cursor[eac], 1ULL)] = make_int2(eab, ebc);
                     pairs[atomicAdd(&cursor[ebc], 1ULL)] = make_int2(eab, eac);
                 }
@@ -233,14 +240,19 @@ __global__ void k_triangles(long long M, const long long *ooff, const int *otgt,
                 ++pb;
             }
         }
+        if (!FILL) {
+            own_cnt[eab] = own;                // each edge is one oriented edge
+            if (own) atomicAdd(&cnt[eab], own);
+        }
     }
 }
 
-__global__ void k_copy_i64(long long n, const long long *src, unsigned long long *dst)
+// each edge's cursor: the start of its pair list past its own pairs
+__global__ void k_cursor_init(long long n, const long long *ioff, const int *own_cnt, unsigned long long *cursor)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x)
-        dst[i] = (unsigned long long)src[i];
+        cursor[i] = (unsigned long long)(ioff[i] + own_cnt[i]);
 }
 
 // ---- binning (terms per item) and renumbering ----
@@ -683,6 +695,20 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     // ---- common-neighbour tables (original edge ids) -------------------------
     DevBuf<long long> d_ioff_old, d_scan_tmp;
     DevBuf<int2> d_pairs_old;
+    // the oriented rows of the triangle listing, alive until its fill is joined
+    DevBuf<int> d_ocnt, d_otgt, d_oeid, d_osrc, d_own;
+    DevBuf<long long> d_ooff;
+    DevBuf<unsigned long long> d_cursor;
+    // Declared after the buffers the side-stream fill reads, so that on an
+    // early return it waits for the fill before they are freed.
+    struct SideFill {
+        cudaStream_t side;
+        bool pending = false;
+        ~SideFill()
+        {
+            if (pending) cudaStreamSynchronize(side);
+        }
+    } fill{ctx.side};
     DRESS_TRY(d_ioff_old.alloc((size_t)E + 1, st));
     DRESS_TRY(d_scan_tmp.alloc(scan_tmp_elems((long long)(S > E ? S : E) + N + 1), st));
     long long T = 0;
@@ -706,9 +732,6 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         count_launch(), k_given_pairs<<<eg, 256, 0, st>>>(E, d_io.get(), d_ux.get(), d_vx.get(), d_ioff_old.get(),
                                           d_pairs_old.get(), d_flags.get());
     } else if (g->variant == DRESS_VARIANT_UNDIRECTED && !dup) {
-        DevBuf<int> d_ocnt, d_otgt, d_oeid, d_osrc;
-        DevBuf<long long> d_ooff;
-        DevBuf<unsigned long long> d_cursor;
         DRESS_TRY(d_ocnt.alloc((size_t)N, st));
         DRESS_TRY(d_ooff.alloc((size_t)N + 1, st));
         DRESS_TRY(d_otgt.alloc((size_t)(S > 0 ? S : 1), st));
@@ -724,16 +747,25 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
         DRESS_CUDA_TRY(cudaMemsetAsync(d_cnt.get(), 0, (size_t)E * sizeof(int), st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         const int tg = (int)grid_for(M, 256, 64 * sms);
+        DRESS_TRY(d_own.alloc((size_t)(E > 0 ? E : 1), st));
+        DRESS_CUDA_TRY(cudaMemsetAsync(d_own.get(), 0, (size_t)E * sizeof(int), st));   // self loops are never oriented
         count_launch(), k_triangles<false><<<tg, 256, 0, st>>>(M, d_ooff.get(), d_otgt.get(), d_oeid.get(), d_osrc.get(),
-                                               d_cnt.get(), nullptr, nullptr);
+                                               d_cnt.get(), d_own.get(), nullptr, nullptr, nullptr);
         DRESS_TRY(exclusive_scan_i32(d_cnt.get(), d_ioff_old.get(), E, d_scan_tmp.get(), st));
         DRESS_CUDA_TRY(counted_memcpy(&T, d_ioff_old.get() + E, sizeof(T), cudaMemcpyDeviceToHost, st));
         DRESS_CUDA_TRY(cudaStreamSynchronize(st));
         DRESS_TRY(d_pairs_old.alloc((size_t)(T > 0 ? T : 1), st));
         DRESS_TRY(d_cursor.alloc((size_t)E, st));
-        count_launch(), k_copy_i64<<<eg, 256, 0, st>>>(E, d_ioff_old.get(), d_cursor.get());
-        count_launch(), k_triangles<true><<<tg, 256, 0, st>>>(M, d_ooff.get(), d_otgt.get(), d_oeid.get(), d_osrc.get(),
-                                              nullptr, d_cursor.get(), d_pairs_old.get());
+        count_launch(), k_cursor_init<<<eg, 256, 0, st>>>(E, d_ioff_old.get(), d_own.get(), d_cursor.get());
+        // The fill runs on the side stream, beside the edge validation, the
+        // bins and the edge renumbering, which need only the counts; the main
+        // stream joins it before the first read of the pairs (k_new_pairs).
+        DRESS_CUDA_TRY(cudaEventRecord(ctx.fork, st));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
+        fill.pending = true;
+        count_launch(), k_triangles<true><<<tg, 256, 0, ctx.side>>>(M, d_ooff.get(), d_otgt.get(), d_oeid.get(),
+                                                                    d_osrc.get(), nullptr, nullptr, d_ioff_old.get(),
+                                                                    d_cursor.get(), d_pairs_old.get());
     } else {
         count_launch(), k_merge_intercepts<false><<<eg, 256, 0, st>>>(E, d_U.get(), d_V.get(), d_off.get(), d_tgt.get(),
                                                        d_eidx.get(), d_cnt.get(), nullptr, nullptr);
@@ -923,6 +955,13 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     }
     ec.list = d_elist.get();
     DRESS_TRY(d_pairs.alloc((size_t)(T > 0 ? T : 1), st));
+    if (fill.pending) {                      // the pairs of the triangle listing are complete
+        DRESS_CUDA_TRY(cudaEventRecord(ctx.join, ctx.side));
+        DRESS_CUDA_TRY(cudaStreamWaitEvent(st, ctx.join, 0));
+        fill.pending = false;
+        d_otgt.release(); d_oeid.release(); d_osrc.release(); d_ooff.release(); d_ocnt.release();
+        d_cursor.release(); d_own.release();
+    }
     if (E - e0 > 0) {
         const int c1 = ec.cls[1], c6 = ec.cls[6];
         if (c1 > 0)
