@@ -851,7 +851,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
                                                         d_cnt.get(), vbits, k0.get(), v0.get());
         unsigned long long *sk = nullptr;
         unsigned *sv = nullptr;
-        DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), E, &sk, &sv, st, sms));
+        DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), E, &sk, &sv, st, sms, 2 * vbits + 1));
         count_launch(), k_inverse<<<eg, 256, 0, st>>>(E, sv, d_eperm.get(), d_einv.get());
     }
     // block items largest first, so the longest sums start first (the sort
@@ -935,7 +935,7 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
                                                                                     v0.get());
             unsigned long long *sk = nullptr;
             unsigned *sv = nullptr;
-            DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), m, &sk, &sv, st, sms));
+            DRESS_TRY(sort_pairs(k0.get(), k1.get(), v0.get(), v1.get(), m, &sk, &sv, st, sms, 3));
             count_launch(), k_class_bounds<<<1, 32, 0, st>>>(m, sk, d_bounds.get());
             DRESS_CUDA_TRY(cudaMemcpyAsync(d_elist.get(), sv, (size_t)m * sizeof(int), cudaMemcpyDeviceToDevice, st));
             DRESS_CUDA_TRY(counted_memcpy(ec.cls, d_bounds.get(), 7 * sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -298,9 +298,11 @@ struct SortPlan {
 // ordered: keys are raw double bits, sorted by value through their
 // order-preserving image (left in place); otherwise they are unsigned
 // integers.  vals/valt (nullable): a 32-bit payload moved with the keys.
+// key_bits < 64: the keys are below 2^key_bits, so only the passes over those
+// bits run, each unconditionally (no host check of whether it moves keys).
 Status sort_segments(unsigned long long *keys, unsigned long long *alt, const std::vector<long long> &begin,
                      const std::vector<long long> &len, SortPlan &sp, cudaStream_t st, int sms,
-                     bool ordered = true, unsigned *vals = nullptr, unsigned *valt = nullptr)
+                     bool ordered = true, unsigned *vals = nullptr, unsigned *valt = nullptr, int key_bits = 64)
 {
     const int nseg = (int)begin.size();
     sp.nseg = nseg;
@@ -353,10 +355,12 @@ Status sort_segments(unsigned long long *keys, unsigned long long *alt, const st
     const int nch = (nt + OFF_CHUNK - 1) / OFF_CHUNK;
     DevBuf<long long> d_csum;
     if (chunked) DRESS_TRY(d_csum.alloc((size_t)nch * RADIX, st));
-    for (int pass = 0; pass < 8; ++pass) {
+    const bool check = key_bits >= 64;
+    const int passes = check ? 8 : std::max(1, (key_bits + 7) / 8);
+    for (int pass = 0; pass < passes; ++pass) {
         int shift = 8 * pass;
         count_launch(), k_tile_hist<<<nt, HT, 0, st>>>(sp.tiles.get(), a, shift, d_counts.get());
-        DRESS_CUDA_TRY(cudaMemsetAsync(d_moves.get(), 0, sizeof(int), st));
+        if (check) DRESS_CUDA_TRY(cudaMemsetAsync(d_moves.get(), 0, sizeof(int), st));
         if (chunked) {
             count_launch(), k_chunk_sums<<<nch, RADIX, 0, st>>>(nt, d_counts.get(), d_csum.get());
             count_launch(), k_chunk_bases<<<1, RADIX, 0, st>>>(nch, sp.seg_begin.get(), d_csum.get(), d_moves.get());
@@ -365,10 +369,12 @@ Status sort_segments(unsigned long long *keys, unsigned long long *alt, const st
             count_launch(), k_seg_offsets<<<nseg, RADIX, 0, st>>>(sp.seg_begin.get(), d_seg_tile0.get(),
                                                                   d_counts.get(), d_offs.get(), d_moves.get());
         }
-        int moves = 0;
-        DRESS_CUDA_TRY(counted_memcpy(&moves, d_moves.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
-        DRESS_CUDA_TRY(cudaStreamSynchronize(st));
-        if (!moves) continue;
+        if (check) {
+            int moves = 0;
+            DRESS_CUDA_TRY(counted_memcpy(&moves, d_moves.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+            DRESS_CUDA_TRY(cudaStreamSynchronize(st));
+            if (!moves) continue;
+        }
         count_launch(), k_tile_scatter<<<nt, HT, 0, st>>>(sp.tiles.get(), a, b, shift, d_offs.get(), pa, pb);
         unsigned long long *t = a;
         a = b;
@@ -395,11 +401,11 @@ Status segmented_sort(unsigned long long *keys, unsigned long long *alt, const s
 }
 
 Status sort_pairs(unsigned long long *keys, unsigned long long *alt, unsigned *vals, unsigned *valt, long long n,
-                  unsigned long long **sorted_keys, unsigned **sorted_vals, cudaStream_t st, int sms)
+                  unsigned long long **sorted_keys, unsigned **sorted_vals, cudaStream_t st, int sms, int key_bits)
 {
     SortPlan sp;
     DRESS_TRY(sort_segments(keys, alt, std::vector<long long>{0}, std::vector<long long>{n}, sp, st, sms, false,
-                            vals, valt));
+                            vals, valt, key_bits));
     *sorted_keys = sp.out;
     *sorted_vals = sp.pout;
     return Status::Ok();

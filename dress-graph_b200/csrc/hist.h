@@ -32,9 +32,11 @@ Status histogram_fetch(HistResult &res, std::vector<int64_t *> &outs, std::vecto
 
 // Stable ascending sort of n unsigned 64-bit keys with a 32-bit payload
 // (LSD radix, 8-bit digits; digits equal on every key are skipped).  The
-// results are in whichever buffer of each pair the last pass wrote.
+// results are in whichever buffer of each pair the last pass wrote.  Keys
+// known to be below 2^key_bits take only the passes over those bits.
 Status sort_pairs(unsigned long long *keys, unsigned long long *alt, unsigned *vals, unsigned *valt, long long n,
-                  unsigned long long **sorted_keys, unsigned **sorted_vals, cudaStream_t st, int sms);
+                  unsigned long long **sorted_keys, unsigned **sorted_vals, cudaStream_t st, int sms,
+                  int key_bits = 64);
 
 // Sorts each segment [begin[s], begin[s]+len[s]) of `keys` (raw double bits,
 // replaced by their order-preserving image, see ordered_to_double) ascending;
