@@ -203,11 +203,13 @@ __global__ void k_orient_fill(int N, const int *off, const int *tgt, const int *
 // A common c closes the triangle {a,b,c}; each of its three edges receives
 // the pair of the other two (the order inside a pair is irrelevant: the term
 // is their sum).
-template <bool FILL>
 // The pairs an oriented edge finds for itself go to the head of its own list
 // (own[eab] of them, counted in the first pass), without atomics; the pairs
 // it finds for its triangles' other two edges go through their cursors,
-// which start after those heads.
+// which start after those heads.  Two rows of very different lengths are
+// intersected by binary searches of the short row's ids in the long one
+// (a merge walk would step through the whole long row).
+template <bool FILL>
 __global__ void k_triangles(long long M, const long long *ooff, const int *otgt, const int *oeid,
                             const int *osrc, int *cnt, int *own_cnt, const long long *ioff,
                             unsigned long long *cursor, int2 *pairs)
@@ -219,25 +221,50 @@ __global__ void k_triangles(long long M, const long long *ooff, const int *otgt,
         long long pb = ooff[b], pb_end = ooff[b + 1];
         int own = 0;                           // this edge's triangles so far
         const long long head = FILL ? ioff[eab] : 0;
-        while (pa < pa_end && pb < pb_end) {
-            int x = otgt[pa], y = otgt[pb];
-            if (x == y) {
-                int eac = oeid[pa], ebc = oeid[pb];
-                if (!FILL) {
-                    ++own;
-                    atomicAdd(&cnt[eac], 1);
-                    atomicAdd(&cnt[ebc], 1);
-                } else {
-                    pairs[head + own++] = make_int2(eac, ebc);
-                    pairs[atomicAdd(&cursor[eac], 1ULL)] = make_int2(eab, ebc);
-                    pairs[atomicAdd(&cursor[ebc], 1ULL)] = make_int2(eab, eac);
-                }
-                ++pa;
-                ++pb;
-            } else if (x < y) {
-                ++pa;
+        auto found = [&](int eac, int ebc) {
+            if (!FILL) {
+                ++own;
+                atomicAdd(&cnt[eac], 1);
+                atomicAdd(&cnt[ebc], 1);
             } else {
-                ++pb;
+                pairs[head + own++] = make_int2(eac, ebc);
+                pairs[atomicAdd(&cursor[eac], 1ULL)] = make_int2(eab, ebc);
+                pairs[atomicAdd(&cursor[ebc], 1ULL)] = make_int2(eab, eac);
+            }
+        };
+        const long long la = pa_end - pa, lb = pb_end - pb;
+        const long long ls = la < lb ? la : lb, ll = la < lb ? lb : la;
+        if (ls > 0 && ls * (64 - __clzll(ll)) < ll) {
+            const bool a_short = la <= lb;
+            const long long s0 = a_short ? pa : pb, s1 = a_short ? pa_end : pb_end;
+            long long lo = a_short ? pb : pa;
+            const long long l1 = a_short ? pb_end : pa_end;
+            for (long long i = s0; i < s1 && lo < l1; ++i) {
+                const int x = otgt[i];
+                long long L = lo, R = l1;              // first id >= x in the long row
+                while (L < R) {
+                    const long long mid = (L + R) >> 1;
+                    if (otgt[mid] < x) L = mid + 1;
+                    else R = mid;
+                }
+                lo = L;
+                if (L < l1 && otgt[L] == x) {
+                    found(oeid[a_short ? i : L], oeid[a_short ? L : i]);
+                    ++lo;
+                }
+            }
+        } else {
+            while (pa < pa_end && pb < pb_end) {
+                int x = otgt[pa], y = otgt[pb];
+                if (x == y) {
+                    found(oeid[pa], oeid[pb]);
+                    ++pa;
+                    ++pb;
+                } else if (x < y) {
+                    ++pa;
+                } else {
+                    ++pb;
+                }
             }
         }
         if (!FILL) {
