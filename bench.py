@@ -416,17 +416,21 @@ def bench_single_fit(args, torch):
             continue
         g = db.Graph(n, U, V, W)
         S = int(g.ptr.contents.adj_offset[n])
-        if label == variants[0]:
-            # an untimed first fit grows the device memory pool and pins the
-            # stage, as a serving process has done before its requests
-            db.fit_graph(g, 1, 1e-6)
+        # an untimed one-sweep fit of the same graph first: it grows the device
+        # memory pool to this variant's buffer sizes and pins the stages, as a
+        # serving process has done before its requests
+        db.fit_graph(g, 1, 1e-6)
+        # three timed fits (one for profiling runs), each from the initial
+        # values; the figures are the fit of median end-to-end time
+        runs = []
+        for _ in range(1 if args.single_fit_only else 3):
             _reset_edges(g)
-        db.counters(reset=True)
-        t0 = time.perf_counter()
-        it, dl = db.fit_graph(g, 100, 1e-6)
-        wall = time.perf_counter() - t0
-        cnt = db.counters()
-        st = db.last_fit_stats()
+            db.counters(reset=True)
+            t0 = time.perf_counter()
+            it, dl = db.fit_graph(g, 100, 1e-6)
+            runs.append((time.perf_counter() - t0, db.counters(), db.last_fit_stats(), it, dl))
+        setups = [r[2]["setup_ms"] for r in runs]
+        wall, cnt, st, it, dl = sorted(runs, key=lambda r: r[0])[len(runs) // 2]
         sweeps = st["sweeps"]
         sweep_ms = st["iterate_ms"] / max(1, sweeps)
         # algorithmic bytes per sweep: 24N + 12S + 48E weighted, 24N + 12S + 32E unweighted
@@ -438,6 +442,7 @@ def bench_single_fit(args, torch):
             "edge_iters_per_s": E * sweeps / (st["iterate_ms"] / 1e3),
             "edge_iters_per_s_e2e": E * sweeps / wall,
             "sweep_ms": sweep_ms, "setup_ms": st["setup_ms"], "e2e_ms": wall * 1e3, "phases_ms": st["phases_ms"],
+            "timed_fits": len(runs), "setup_ms_range": [min(setups), max(setups)],
             "h2d_bytes": cnt["h2d_bytes"], "d2h_bytes": cnt["d2h_bytes"], "launches": cnt["launches"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
