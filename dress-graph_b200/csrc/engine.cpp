@@ -36,30 +36,40 @@ void set_last_error(const Status &s)
 Pinned::~Pinned()
 {
     if (base_) cudaFreeHost(base_);
+    for (char *r : retired_) cudaFreeHost(r);
 }
 
 Status Pinned::reserve(size_t bytes)
 {
     if (bytes <= cap_) return Status::Ok();
-    // Pinning host memory is slow and freeing it waits for the device, so
-    // the buffer grows at least twofold (and to at least 32 MiB): a stream
-    // of growing requests reallocates it a few times, not at every request.
+    // Pinning host memory is slow, so the buffer grows at least twofold (and
+    // to at least 32 MiB): a stream of growing requests reallocates it a few
+    // times, not at every request.  Freeing pinned memory waits for the whole
+    // device -- every stream of every lane -- so an outgrown buffer is kept
+    // until the owner goes away (at most the final size again, the growth
+    // being geometric); only when pinning fails are the old buffers freed
+    // and the allocation retried.
     const size_t want = std::max(bytes, std::max(2 * cap_, (size_t)32 << 20));
-    if (base_) cudaFreeHost(base_);
-    base_ = nullptr;
-    cap_ = 0;
-    if (cudaMallocHost((void **)&base_, want) == cudaSuccess) {
-        cap_ = want;
+    char *nb = nullptr;
+    if (cudaMallocHost((void **)&nb, want) != cudaSuccess) {
+        cudaGetLastError();
+        nb = nullptr;
+        if (base_) cudaFreeHost(base_);
+        for (char *r : retired_) cudaFreeHost(r);
+        retired_.clear();
+        base_ = nullptr;
+        cap_ = 0;
+        if (cudaMallocHost((void **)&nb, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return Status::Err(DRESSX_ENOMEM, "pinned host allocation failed");
+        }
+        base_ = nb;
+        cap_ = bytes;
         return Status::Ok();
     }
-    cudaGetLastError();
-    base_ = nullptr;
-    if (cudaMallocHost((void **)&base_, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        base_ = nullptr;
-        return Status::Err(DRESSX_ENOMEM, "pinned host allocation failed");
-    }
-    cap_ = bytes;
+    if (base_) retired_.push_back(base_);
+    base_ = nb;
+    cap_ = want;
     return Status::Ok();
 }
 

@@ -91,6 +91,7 @@ class Pinned {
   private:
     char *base_ = nullptr;
     size_t cap_ = 0;
+    std::vector<char *> retired_;          // outgrown buffers, freed with the owner
 };
 
 // ---- an execution context: where one stream of work runs ------------------

@@ -369,7 +369,10 @@ Status Server::start(const dressx_server_config_t *c)
         DRESS_TRY(c2->create(device, sms, &en.cfg, hi));
     }
     // staging buffers pinned now rather than while requests are in flight
-    for (Lane *ln : lanes) ln->ctx.stage->reserve(STAGE_START_BYTES);
+    for (Lane *ln : lanes) {
+        ln->ctx.stage->reserve(STAGE_START_BYTES);
+        ln->ctx.stage2->reserve(2 * STAGE_CHUNK);    // the second upload of a large fit
+    }
     for (Ctx *c2 : fins) c2->stage->reserve(STAGE_START_BYTES);
     t0 = Clock::now();
     threads.emplace_back([this] { scheduler(); });
