@@ -494,6 +494,66 @@ __global__ void __launch_bounds__(SORT_BLK_THR) k_sort_pairs_blk(const int *list
     }
 }
 
+// Each row's slots in edge-id order, in place, so that a vertex's owned
+// edges (one contiguous id run each in the two edge parts) are neighbouring
+// slots: their gathers in the vertex phase read neighbouring products.  Rows
+// of vertices [lo, hi), which all have n slots of one size class; rows past
+// BIG_CAP slots keep their order.
+__global__ void k_sort_rows_thr(int lo, int hi, const long long *row_off, int *row_eid)
+{
+    for (int i = lo + blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += gridDim.x * blockDim.x) {
+        const long long b = row_off[i];
+        const int n = (int)(row_off[i + 1] - b);
+        int w[16];
+        for (int k = 0; k < n && k < 16; ++k) {
+            const int t = row_eid[b + k];
+            int j = k;
+            for (; j > 0 && w[j - 1] > t; --j) w[j] = w[j - 1];
+            w[j] = t;
+        }
+        for (int k = 0; k < n && k < 16; ++k) row_eid[b + k] = w[k];
+    }
+}
+
+__global__ void __launch_bounds__(32 * SORT_WARPS) k_sort_rows_warp(int lo, int hi, const long long *row_off,
+                                                                    int *row_eid)
+{
+    __shared__ unsigned long long sb[SORT_WARPS][SORT_WARP_CAP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long *buf = sb[wid];
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int i = lo + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < hi; i += nw) {
+        const long long b = row_off[i];
+        const int n = (int)(row_off[i + 1] - b);
+        if (n > SORT_WARP_CAP) continue;
+        int P = 32;
+        while (P < n) P <<= 1;
+        for (int k = lane; k < P; k += 32) buf[k] = k < n ? (unsigned long long)(unsigned)row_eid[b + k] : ~0ULL;
+        __syncwarp();
+        bitonic<false>(buf, P, lane, 32);
+        for (int k = lane; k < n; k += 32) row_eid[b + k] = (int)(unsigned)buf[k];
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(SORT_BLK_THR) k_sort_rows_blk(int lo, int hi, const long long *row_off, int *row_eid)
+{
+    __shared__ unsigned long long buf[BIG_CAP];
+    for (int i = lo + (int)blockIdx.x; i < hi; i += gridDim.x) {
+        const long long b = row_off[i];
+        const int n = (int)(row_off[i + 1] - b);
+        if (n > BIG_CAP) continue;
+        int P = 32;
+        while (P < n) P <<= 1;
+        for (int k = threadIdx.x; k < P; k += blockDim.x)
+            buf[k] = k < n ? (unsigned long long)(unsigned)row_eid[b + k] : ~0ULL;
+        __syncthreads();
+        bitonic<true>(buf, P, threadIdx.x, blockDim.x);
+        for (int k = threadIdx.x; k < n; k += blockDim.x) row_eid[b + k] = (int)(unsigned)buf[k];
+        __syncthreads();
+    }
+}
+
 __global__ void k_gather_seg(int n, const int *perm, const int *len, int *out)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = len[perm[i]];
@@ -922,6 +982,18 @@ Status fit_graph(p_dress_graph_t g, int max_iterations, double epsilon, int *ite
     count_launch(), k_new_rows<<<grid_for((long long)N * 32, 256, 64 * sms), 256, 0, st>>>(
         N, d_vperm.get(), d_off.get(), d_eidx.get(), d_einv.get(), d_row_off.get(), d_row_eid.get(),
         d_nw.get(), d_nwi.get());
+    if (locality) {                          // rows in edge-id order (vertex bins: thread, warp, block)
+        const int t0 = vb.start[B2], t1 = vb.start[BMED], w1 = vb.start[BBLOCK], b1 = vb.start[BBIG];
+        if (t1 > t0)
+            count_launch(), k_sort_rows_thr<<<grid_for(t1 - t0, 256, 64 * sms), 256, 0, st>>>(t0, t1, d_row_off.get(),
+                                                                                          d_row_eid.get());
+        if (w1 > t1)
+            count_launch(), k_sort_rows_warp<<<grid_for((long long)(w1 - t1) * 32, 32 * SORT_WARPS, 32 * sms),
+                                               32 * SORT_WARPS, 0, st>>>(t1, w1, d_row_off.get(), d_row_eid.get());
+        if (b1 > w1)
+            count_launch(), k_sort_rows_blk<<<(unsigned)std::min(b1 - w1, 8 * sms), SORT_BLK_THR, 0, st>>>(
+                w1, b1, d_row_off.get(), d_row_eid.get());
+    }
     d_eidx.release();
     d_ndeg.release();
 
