@@ -66,7 +66,7 @@ KBATCH_HEADLINE_NCU = {"dram_bytes": 19.33e6 + 190.33e6,
 # The 28M-edge single fit: dram__bytes_read.sum + dram__bytes_write.sum of the
 # twelve sweep kernels of one sweep (sweep 10), one capture per variant
 # (profiles/single_fit_chunglu28m_sweep_dram.md)
-SINGLE_FIT_NCU = {"edges": 28_000_000, "weighted": 4.286e9 + 0.512e9, "unweighted": 3.925e9 + 0.286e9}
+SINGLE_FIT_NCU = {"edges": 28_000_000, "weighted": 4.218e9 + 0.512e9, "unweighted": 3.858e9 + 0.283e9}
 
 
 def parse():

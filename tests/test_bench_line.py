@@ -14,13 +14,13 @@ def _fit(sweep_ms, frac, traffic=None, dram_frac=None):
 
 
 def test_single_fit_fractions_and_traffic():
-    single = {"weighted": _fit(1.53, 0.2116, 4.798e9, 0.481),
+    single = {"weighted": _fit(1.53, 0.2116, 4.730e9, 0.481),
               "unweighted": _fit(1.44, 0.1768),
               "cpu_baseline": {"omp": {"ms_per_sweep": 11412.0}}}
     out = bench.compact_sections(single, None, None, None)
     sf = out["single_fit"]
     assert sf["weighted"]["hbm_frac"] == 0.212 and sf["weighted"]["sweep_ms"] == 1.53
-    assert sf["weighted"]["traffic_gb"] == 4.8 and sf["weighted"]["dram_frac"] == 0.481
+    assert sf["weighted"]["traffic_gb"] == 4.73 and sf["weighted"]["dram_frac"] == 0.481
     # no capture for this size: no traffic keys rather than a made-up figure
     assert "traffic_gb" not in sf["unweighted"] and "dram_frac" not in sf["unweighted"]
     assert sf["cpu_omp_ms_per_sweep"] == 11400.0
